@@ -1,0 +1,343 @@
+"""Benchmark: split-step Strang steps/s of the real-time stirred 256^3 complex64 solve.
+
+One "step" is one Strang step of the hot path (local half-step, 3-D FFT,
+kinetic phase, inverse 3-D FFT, local half-step) over the whole 256^3 grid.
+
+Workload ("large single solve", 256^3 complex64): trap V = (x^2 + 1.44 y^2 +
+2.25 z^2)/2, box [-12,12)^3, g = 2000, dt = 2.5e-4 (oscillator units), rotating
+Gaussian beam A = 10, w = 0.5, R = 2, angular rate ramped 0 -> 0.5 over the first
+200 steps.  The plan runs in the reference's units (V x2, g x2, dt /2), which is
+an exact reparametrisation.  Inputs are synthetic (seeded noisy Gaussian relaxed
+for 50 imaginary-time steps); psi is 128 MiB, larger than the 126 MB L2.
+
+``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]``
+prints one JSON line (rank 0).  Multi-GPU runs are independent replicas (one
+solve per GPU, weak scaling); ``value`` is the whole-job steps/s.
+"""
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_GRID, L_BOX, G, DT = 256, 24.0, 2000.0, 2.5e-4
+BEAM = dict(amp=10.0, width=0.5, radius=2.0, omega=0.5, ramp_steps=200)
+TRAP_REF = "x**2+1.44*y**2+2.25*z**2"
+METRIC = "steps/s & HBM roofline % at 256^3 c64"
+WORKLOAD = ("stir256_c64: real-time stirred GPE, 256^3 complex64, box [-12,12)^3, g=2000, "
+            "dt=2.5e-4, beam A=10 w=0.5 R=2 Omega 0->0.5 over 200 steps")
+FALLBACK_HBM = 6650.0
+
+
+def measured_peak():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        try:
+            return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return FALLBACK_HBM, "fallback"
+
+
+# ------------------------------------------------------------------ distributed
+def dist_init(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if os.environ.get("GPE_BENCH_BACKEND", "nccl") == "nccl" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(value, world, device=None):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world, device=None):
+    if world > 1:
+        import torch.distributed as dist
+        if device is not None:
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """``nvidia-smi`` clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ workload
+def grids():
+    x = np.linspace(-L_BOX / 2, L_BOX / 2, N_GRID, endpoint=False)
+    k = 2 * np.pi * np.fft.fftfreq(N_GRID, L_BOX / N_GRID)
+    return x, k
+
+
+def initial_state(x, seed=0):
+    """Seeded noisy Gaussian, normalised (host, complex128)."""
+    n = len(x)
+    rng = np.random.default_rng(seed)
+    g = np.exp(-x ** 2 / 2)
+    psi = (g[:, None, None] * g[None, :, None] * g[None, None, :]).astype(np.complex128)
+    psi *= 1 + 0.01 * (rng.standard_normal((n, n, n)) + 1j * rng.standard_normal((n, n, n))) / np.sqrt(2)
+    dx = x[1] - x[0]
+    psi /= np.sqrt(np.sum(np.abs(psi) ** 2) * dx ** 3)
+    return psi
+
+
+def ours(args, world, rank, local):
+    import torch
+    from gpe_simulator_b200 import beam_in_reference_units, build
+    from gpe_simulator_b200.plan import Plan, launch_count, profile, profile_read
+    build.build()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    x, k = grids()
+    beam = beam_in_reference_units(BEAM["amp"], BEAM["width"], BEAM["radius"], BEAM["omega"],
+                                   BEAM["ramp_steps"] * DT)
+    plan = Plan(N_GRID, x, k, dtype=torch.complex64, kind="real", beta=2 * G, dt=DT / 2,
+                static_expr=TRAP_REF, beam=beam)
+    prep = Plan(N_GRID, x, k, dtype=torch.complex64, kind="imaginary", beta=2 * G, dt=DT,
+                static_expr=TRAP_REF)
+    host0 = initial_state(x, seed=rank).astype(np.complex64)
+    psi = torch.from_numpy(host0).to(device)
+    prep.step(psi, 50)
+    plan.step(psi, args.warmup, 0)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K steps, one multi-step C-ABI call, inputs resident in HBM
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.6)
+    n0 = launch_count(plan)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world, device)
+    torch.cuda.synchronize()
+    start.record()
+    plan.step(psi, args.steps, args.warmup)
+    end.record()
+    torch.cuda.synchronize()
+    barrier(world, device)
+    launches = launch_count(plan) - n0
+    ms = start.elapsed_time(end)
+    clocks = sampler.stop()
+    ms_max = max_over_ranks(ms, world, device)
+    value = world * args.steps / (ms_max / 1e3)
+
+    # ---- per-launch durations of the sweeps (events around each launch, same stream)
+    profile(plan, True)
+    plan.step(psi, args.steps, args.warmup + args.steps)
+    per = profile_read(plan)
+    profile(plan, False)
+    torch.cuda.synchronize()
+    dom = max(per, key=lambda a: per[a][0])
+    dom_ms, dom_n = per[dom]
+    s_bytes = 8
+    m = N_GRID ** 3
+    bytes_per_launch = 2 * s_bytes * m
+    achieved = bytes_per_launch / (dom_ms / dom_n / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(f"sweep_{dom}")
+
+    # ---- end to end: public closure API with host buffers, H2D + D2H every step
+    from gpe_simulator_b200.make_propagator import make_real_propagator
+    from types import SimpleNamespace
+    from gpe_simulator_b200.expressions import cuda_expression
+    st = SimpleNamespace(
+        type="real", N_grids=N_GRID, beta=2 * G, dt=DT / 2, beam=beam, kinetic_coeff=1.0,
+        x_array=torch.from_numpy(x).to(device), k_array=torch.from_numpy(k).to(device),
+        staticV=torch.zeros((N_GRID,) * 3, dtype=torch.complex128, device=device),
+        potential_params=dict(static=dict(activate=True, expression=cuda_expression(TRAP_REF)),
+                              dynamic=dict(activate=False, expression="0")),
+        k_cut_params=dict(activate=False, k_cut=0.0), psi=psi)
+    prop = make_real_propagator(st)
+    host = torch.from_numpy(host0).pin_memory()
+    out_host = torch.empty_like(host).pin_memory()
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    prop(st, 0.0)
+    torch.cuda.synchronize()
+    barrier(world, device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(e2e_steps):
+        st.psi.copy_(host, non_blocking=True)
+        prop(st, (args.warmup + i) * st.dt)
+        out_host.copy_(st.psi, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, device)
+    e2e = world * e2e_steps / (e2e_ms / 1e3)
+    nbytes = host.numel() * host.element_size()
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic (seeded noisy Gaussian relaxed 50 imaginary steps)",
+        "config": {"workload": WORKLOAD, "grid": N_GRID, "psi_bytes": nbytes,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (128 MiB psi vs 126 MB L2), no flush"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": f"k_sweep axis {dom}",
+                     "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "avg_launch_ms": dom_ms / dom_n,
+                     "per_axis_ms": {a: per[a][0] / max(per[a][1], 1) for a in per}},
+        "step_roofline": {"algorithmic_bytes_per_step": 6 * s_bytes * m,
+                          "achieved_gbs": 6 * s_bytes * m * value / world / 1e9,
+                          "frac": 6 * s_bytes * m * value / world / 1e9 / peak},
+        "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes, "steps": e2e_steps,
+                "path": "make_real_propagator closure per step, psi H2D from pinned host before "
+                        "and D2H after every step"},
+        "clocks": clocks,
+    }
+    if world == 1 and rank == 0 and not args.no_cpu:
+        result["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+    return result, plan
+
+
+def cpu_baseline(budget_s, steps_cap=None):
+    """The oracle port (NumPy + scipy.fft, all host threads) on the same workload."""
+    from oracle import ssf
+    from oracle.ssf import Beam, Model
+    x, _ = grids()
+    b = Beam(2 * BEAM["amp"], BEAM["width"], BEAM["radius"], 2 * BEAM["omega"],
+             BEAM["ramp_steps"] * DT / 2)
+    model = Model(n=N_GRID, simulation_range=L_BOX, kind="real", beta=2 * G, dt=DT / 2,
+                  static_expr=TRAP_REF, beam=b)
+    psi = initial_state(x).astype(np.complex64)
+    t0 = time.perf_counter()
+    psi = ssf.step(psi, model, 0.0)
+    one = time.perf_counter() - t0
+    n = max(1, int(budget_s / max(one, 1e-3)))
+    if steps_cap:
+        n = min(n, steps_cap)
+    t0 = time.perf_counter()
+    for i in range(n):
+        psi = ssf.step(psi, model, (i + 1) * model.dt)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "steps/s", "cores": ssf.WORKERS, "kind": "port",
+            "sample": f"{n} Strang steps of the 256^3 workload in complex64 (oracle port, "
+                      f"scipy.fft workers={ssf.WORKERS}) after 1 untimed step"}
+
+
+def reference(args, world, rank):
+    """The reference arm: the oracle port of the reference algorithm on host cores."""
+    if rank != 0:
+        return None
+    budget = float(os.environ.get("GPE_REFERENCE_SECONDS", "60"))
+    base = cpu_baseline(budget, steps_cap=args.steps)
+    return {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "grid": N_GRID},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=40)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
+        out = reference(args, world, rank)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
+    world, rank, local = dist_init(args.gpus)
+    out, plan = ours(args, world, rank, local)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    plan.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

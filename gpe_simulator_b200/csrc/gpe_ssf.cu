@@ -1,0 +1,784 @@
+// gpe_ssf.cu -- plans, launch sequences and the C ABI (include/gpe_ssf.h).
+#include "../../include/gpe_ssf.h"
+#include "gpe_sweep.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace gpe;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CU(call)                                                                            \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) {                                                                \
+      if (e_ == cudaErrorMemoryAllocation) return fail(GPE_ERR_OOM, cudaGetErrorString(e_)); \
+      return fail(GPE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
+    }                                                                                       \
+  } while (0)
+
+// Host evaluation of a potential program (same semantics as eval_program).
+double host_eval(const std::vector<double>& prog, double x, double y, double z, double t) {
+  double st[GPE_STACK_MAX];
+  int sp = 0;
+  for (size_t pc = 0; pc < prog.size();) {
+    const int op = (int)prog[pc++];
+    switch (op) {
+      case GPE_OP_CONST: st[sp++] = prog[pc++]; break;
+      case GPE_OP_X: st[sp++] = x; break;
+      case GPE_OP_Y: st[sp++] = y; break;
+      case GPE_OP_Z: st[sp++] = z; break;
+      case GPE_OP_T: st[sp++] = t; break;
+      case GPE_OP_ADD: --sp; st[sp - 1] = st[sp - 1] + st[sp]; break;
+      case GPE_OP_SUB: --sp; st[sp - 1] = st[sp - 1] - st[sp]; break;
+      case GPE_OP_MUL: --sp; st[sp - 1] = st[sp - 1] * st[sp]; break;
+      case GPE_OP_DIV: --sp; st[sp - 1] = st[sp - 1] / st[sp]; break;
+      case GPE_OP_POW: --sp; st[sp - 1] = std::pow(st[sp - 1], st[sp]); break;
+      case GPE_OP_NEG: st[sp - 1] = -st[sp - 1]; break;
+      case GPE_OP_SIN: st[sp - 1] = std::sin(st[sp - 1]); break;
+      case GPE_OP_COS: st[sp - 1] = std::cos(st[sp - 1]); break;
+      case GPE_OP_TAN: st[sp - 1] = std::tan(st[sp - 1]); break;
+      case GPE_OP_EXP: st[sp - 1] = std::exp(st[sp - 1]); break;
+      case GPE_OP_SQRT: st[sp - 1] = std::sqrt(st[sp - 1]); break;
+      case GPE_OP_TANH: st[sp - 1] = std::tanh(st[sp - 1]); break;
+      case GPE_OP_ABS: st[sp - 1] = std::fabs(st[sp - 1]); break;
+      case GPE_OP_LOG: st[sp - 1] = std::log(st[sp - 1]); break;
+      default: break;
+    }
+  }
+  return sp ? st[0] : 0.0;
+}
+
+// Validate a program: known opcodes, operands present, stack within bounds, one result.
+bool check_program(const double* p, int len, std::string& why) {
+  if (len == 0) return true;
+  if (!p || len < 0 || len > GPE_PROGRAM_MAX) { why = "program length out of range"; return false; }
+  int sp = 0;
+  for (int pc = 0; pc < len;) {
+    const double opd = p[pc++];
+    const int op = (int)opd;
+    if ((double)op != opd) { why = "non-integer opcode"; return false; }
+    int pop = 0, push = 1;
+    switch (op) {
+      case GPE_OP_CONST:
+        if (pc >= len) { why = "constant without operand"; return false; }
+        ++pc; pop = 0; break;
+      case GPE_OP_X: case GPE_OP_Y: case GPE_OP_Z: case GPE_OP_T: pop = 0; break;
+      case GPE_OP_ADD: case GPE_OP_SUB: case GPE_OP_MUL: case GPE_OP_DIV: case GPE_OP_POW: pop = 2; break;
+      case GPE_OP_NEG: case GPE_OP_SIN: case GPE_OP_COS: case GPE_OP_TAN: case GPE_OP_EXP:
+      case GPE_OP_SQRT: case GPE_OP_TANH: case GPE_OP_ABS: case GPE_OP_LOG: pop = 1; break;
+      default: why = "unknown opcode"; return false;
+    }
+    if (sp < pop) { why = "stack underflow"; return false; }
+    sp = sp - pop + push;
+    if (sp > GPE_STACK_MAX - 1) { why = "expression too deep"; return false; }
+  }
+  if (sp != 1) { why = "program must leave exactly one value"; return false; }
+  return true;
+}
+
+bool factorize(int n, PassPlan& pp) {
+  pp.n = n;
+  pp.npass = 0;
+  int m = n, twos = 0;
+  while (m % 2 == 0) { m /= 2; ++twos; }
+  std::vector<int> r;
+  // powers of two: radix 16 where possible; remainders balanced with 8/4/2
+  int t = twos;
+  if (t % 4 == 1 && t >= 5) { r.push_back(8); r.push_back(4); t -= 5; }
+  else if (t % 4 == 1) { r.push_back(2); t -= 1; }
+  else if (t % 4 == 2) { r.push_back(4); t -= 2; }
+  else if (t % 4 == 3) { r.push_back(8); t -= 3; }
+  while (t >= 4) { r.push_back(16); t -= 4; }
+  const int odd[] = {3, 5, 7, 11, 13};
+  for (int p : odd)
+    while (m % p == 0) { r.push_back(p); m /= p; }
+  if (m != 1) return false;
+  if ((int)r.size() > 12) return false;
+  for (size_t i = 0; i < r.size(); ++i) pp.radix[i] = r[i];
+  pp.npass = (int)r.size();
+  return true;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- small kernels
+namespace gpe {
+
+// d_v[idx] = general static program + Re(staticV) (or the real array), precision R;
+// d_im[idx] = Im(staticV) for a complex staticV (real time).
+template <typename R>
+__global__ void k_build_static(int n, const double* x, const double* prog, int len, const void* v,
+                               int kind, R* out_re, R* out_im) {
+  const long long m = (long long)n * n * n;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < m;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(idx % n), j = (int)((idx / n) % n), i = (int)(idx / ((long long)n * n));
+    double re = 0.0, im = 0.0;
+    if (len) re += eval_program(prog, len, x[i], x[j], x[k], 0.0);
+    if (kind == GPE_V_REAL64) re += ((const double*)v)[idx];
+    if (kind == GPE_V_CPLX128) {
+      const double2 c = ((const double2*)v)[idx];
+      re += c.x;
+      im = c.y;
+    }
+    if (out_re) out_re[idx] = (R)re;
+    if (out_im) out_im[idx] = (R)im;
+  }
+}
+
+// Sum per-block diagnostic partials in a fixed order.
+// out[0..3] = sums of pa columns 0..2 and pb column 3; out[4 + b] = histogram bin b.
+__global__ void k_finish_diag(const double* pa, int na, const double* pb, int nb, const double* hist,
+                              int nbins, double* out) {
+  __shared__ Acc sh[32 * 4];
+  Acc a[4];
+  for (int b = threadIdx.x; b < na; b += blockDim.x) {
+    a[0].add(pa[b * 4 + 0]);
+    a[1].add(pa[b * 4 + 1]);
+    a[2].add(pa[b * 4 + 2]);
+  }
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) a[3].add(pb[b * 4 + 3]);
+  block_merge<4>(a, sh);
+  if (threadIdx.x == 0)
+    for (int v = 0; v < 4; ++v) out[v] = a[v].value();
+  if (hist) {
+    for (int bin = threadIdx.x; bin < nbins; bin += blockDim.x) {
+      Acc h;
+      for (int b = 0; b < nb; ++b) h.add(hist[(long long)b * nbins + bin]);
+      out[4 + bin] = h.value();
+    }
+  }
+}
+
+}  // namespace gpe
+
+// ---------------------------------------------------------------- the plan
+struct gpe_plan {
+  int n = 0, dtype = 0, kind = 0;
+  double beta = 0, dt = 0, ckin = 1, dx = 0;
+  size_t csize = 8;                // bytes per complex element
+  std::vector<double> x, k;
+  std::vector<double> prog_static_g, prog_dyn;
+  PassPlan pp{};
+  Phys ph{};
+  int lt_z = 1, lt_yx = 16;
+  bool gen = false;                // grid size needs the odd-prime radices 7/11/13
+  int ept = 16;                    // elements per thread of the sweep family
+  int nbins = 0;
+  double shell_w = 0;
+  std::vector<long long> counts;
+  // device buffers
+  double* d_x = nullptr;
+  double* d_k = nullptr;
+  double2* d_kin = nullptr;
+  double* d_kth = nullptr;
+  void* d_vax = nullptr;
+  void* d_vre = nullptr;
+  void* d_vim = nullptr;
+  double* d_prog_g = nullptr;
+  double* d_dyn = nullptr;
+  void* d_tw = nullptr;
+  double* d_partial = nullptr;   // 2 areas of 4*max_tiles doubles
+  unsigned* d_ticket = nullptr;
+  double* d_scale = nullptr;     // [sqrtN, 1/sqrtN, N, ...]
+  int* d_status = nullptr;
+  double* d_hist = nullptr;
+  double* d_out = nullptr;       // diag results [4 + nbins]
+  void* d_work = nullptr;        // diagnostic FFT scratch (size of psi), lazily
+  int max_tiles = 0;
+  // launch accounting and optional per-launch timing (events around each sweep)
+  long long launches = 0;
+  bool prof = false;
+  struct Rec { int ax; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+};
+
+namespace {
+
+int tiles_of(const gpe_plan* p, int ax) {
+  const int n = p->n;
+  if (ax == AX_Z) return (n * n + p->lt_z - 1) / p->lt_z;
+  return n * ((n + p->lt_yx - 1) / p->lt_yx);
+}
+
+template <typename R>
+int launch(gpe_plan* p, int ax, Sweep sw, cudaStream_t st) {
+  using C = typename Cx<R>::T;
+  const int n = p->n;
+  sw.pp = p->pp;
+  sw.tw = p->d_tw;
+  sw.tw_lo = (const char*)p->d_tw + (size_t)n * sizeof(C);
+  sw.ticket = p->d_ticket;
+  sw.scale = p->d_scale;
+  sw.status = p->d_status;
+  sw.nbins = p->nbins;
+  sw.shell_w = p->shell_w;
+  int lt = ax == AX_Z ? p->lt_z : p->lt_yx;
+  sw.lt = lt;
+  sw.tiles_per_row = (n + p->lt_yx - 1) / p->lt_yx;
+  const int tiles = tiles_of(p, ax);
+  const int pitch = ax == AX_Z ? ((n & 1) ? n : n + 1) : lt;
+  const int tile_elems = ax == AX_Z ? lt * pitch : n * lt;
+  const int E = n * lt;
+  int threads = (E + p->ept - 1) / p->ept;
+  threads = ((threads + 31) / 32) * 32;
+  if (threads < 32) threads = 32;
+  if (threads > 512) return fail(GPE_ERR_UNSUPPORTED, "tile too large");
+  size_t smem = (size_t)(2 * n + tile_elems) * sizeof(C) + 32 * 4 * sizeof(Acc) + (size_t)p->nbins * sizeof(double);
+  if (smem > 200 * 1024) return fail(GPE_ERR_UNSUPPORTED, "tile does not fit in shared memory");
+  CU(launch_sweep<R>(ax, p->gen, p->ph, sw, tiles, threads, smem, st));
+  CU(cudaGetLastError());
+  return GPE_OK;
+}
+
+cudaEvent_t pooled_event(gpe_plan* p) {
+  if (!p->pool.empty()) {
+    cudaEvent_t e = p->pool.back();
+    p->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+int sweep(gpe_plan* p, int ax, const Sweep& sw, cudaStream_t st) {
+  gpe_plan::Rec r{ax, nullptr, nullptr};
+  if (p->prof) {
+    r.a = pooled_event(p);
+    r.b = pooled_event(p);
+    CU(cudaEventRecord(r.a, st));
+  }
+  const int rc = p->dtype == GPE_C64 ? launch<float>(p, ax, sw, st) : launch<double>(p, ax, sw, st);
+  if (rc == GPE_OK) ++p->launches;
+  if (p->prof) {
+    CU(cudaEventRecord(r.b, st));
+    p->recs.push_back(r);
+  }
+  return rc;
+}
+
+Sweep mk_sweep(const void* src, void* dst) {
+  Sweep s;
+  memset(&s, 0, sizeof(s));
+  s.src = src;
+  s.dst = dst;
+  return s;
+}
+
+// reference: t = i*dt (gpe/launch.py:10), t_mid = t + dt/2 (gpe/make_propagator.py:94)
+double t_mid_host(const gpe_plan* p, long long step) { return (double)step * p->dt + p->dt / 2; }
+
+#define TRY(x) do { int r_ = (x); if (r_ != GPE_OK) return r_; } while (0)
+
+// Norm of psi into d_scale (sqrtN, 1/sqrtN, N) via a no-store sweep.
+int norm_sweep(gpe_plan* p, const void* psi, cudaStream_t st) {
+  Sweep s = mk_sweep(psi, nullptr);
+  s.post = PW_NORM;
+  s.partial = p->d_partial;
+  return sweep(p, AX_Z, s, st);
+}
+
+int scale_sweep(gpe_plan* p, void* psi, cudaStream_t st) {
+  Sweep s = mk_sweep(psi, psi);
+  s.pre = PW_SCALE;
+  return sweep(p, AX_Z, s, st);
+}
+
+int ensure_work(gpe_plan* p) {
+  if (p->d_work) return GPE_OK;
+  const size_t bytes = (size_t)p->n * p->n * p->n * p->csize;
+  CU(cudaMalloc(&p->d_work, bytes));
+  return GPE_OK;
+}
+
+int ensure_hist(gpe_plan* p) {
+  if (p->d_hist) return GPE_OK;
+  const size_t bytes = (size_t)tiles_of(p, AX_X) * p->nbins * sizeof(double);
+  CU(cudaMalloc(&p->d_hist, bytes));
+  return GPE_OK;
+}
+
+int fill_plan(gpe_plan* p, const gpe_desc* d) {
+  const int n = d->n;
+  if (n < 2 || n > 1024) return fail(GPE_ERR_UNSUPPORTED, "n must be in [2, 1024]");
+  if (!factorize(n, p->pp)) return fail(GPE_ERR_UNSUPPORTED, "n has a prime factor larger than 13");
+  if (d->dtype != GPE_C64 && d->dtype != GPE_C128) return fail(GPE_ERR_ARG, "dtype must be GPE_C64 or GPE_C128");
+  if (d->kind != GPE_IMAGINARY && d->kind != GPE_REAL) return fail(GPE_ERR_ARG, "kind must be imaginary or real");
+  if (!d->x_array || !d->k_array) return fail(GPE_ERR_ARG, "x_array and k_array are required");
+  if (!std::isfinite(d->beta) || !std::isfinite(d->dt) || !std::isfinite(d->kinetic_coeff))
+    return fail(GPE_ERR_ARG, "beta, dt and kinetic_coeff must be finite");
+  std::string why;
+  const double* progs[] = {d->static_x, d->static_y, d->static_z, d->static_g, d->dynamic_g};
+  const int lens[] = {d->static_x_len, d->static_y_len, d->static_z_len, d->static_g_len, d->dynamic_g_len};
+  for (int q = 0; q < 5; ++q)
+    if (!check_program(progs[q], lens[q], why)) return fail(GPE_ERR_ARG, "potential program: " + why);
+  if (d->kind == GPE_IMAGINARY && (d->dynamic_g_len || d->beam_enabled || d->k_cut_enabled))
+    return fail(GPE_ERR_ARG, "imaginary time takes no time-dependent potential, beam or cutoff");
+  p->n = n;
+  p->dtype = d->dtype;
+  p->kind = d->kind;
+  p->beta = d->beta;
+  p->dt = d->dt;
+  p->ckin = d->kinetic_coeff;
+  p->csize = d->dtype == GPE_C64 ? 8 : 16;
+  p->x.assign(d->x_array, d->x_array + n);
+  p->k.assign(d->k_array, d->k_array + n);
+  p->dx = p->x[1] - p->x[0];
+  if (d->static_g_len) p->prog_static_g.assign(d->static_g, d->static_g + d->static_g_len);
+  if (d->dynamic_g_len) p->prog_dyn.assign(d->dynamic_g, d->dynamic_g + d->dynamic_g_len);
+  // kernel family and tiles: at most 512 threads x ept elements per tile;
+  // 128-byte rows for y/x tiles, ~4096 elements per z tile
+  for (int q = 0; q < p->pp.npass; ++q)
+    if (p->pp.radix[q] > 5 && p->pp.radix[q] != 8 && p->pp.radix[q] != 16) p->gen = true;
+  p->ept = p->gen ? 8 : 16;
+  const int emax = 512 * p->ept;
+  p->lt_yx = std::max(1, std::min(d->dtype == GPE_C64 ? 16 : 8, emax / n));
+  p->lt_z = std::max(1, std::min(n * n, std::min(4096, emax) / n));
+  // shells (reference gpe/nk_extraction.py:19-21)
+  const double dk = std::fabs(p->k[1] - p->k[0]);
+  if (d->nk_bins > 0) {
+    if (d->nk_bins < 2) return fail(GPE_ERR_ARG, "nk_bins must be >= 2");
+    p->nbins = d->nk_bins;
+    p->shell_w = std::sqrt(3.0) * (n / 2) * dk / (p->nbins - 1);
+  } else {
+    p->nbins = (int)std::floor(std::sqrt(3.0) * (n / 2) + 0.5) + 1;
+    p->shell_w = dk;
+  }
+  p->counts.assign(p->nbins, 0);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j)
+      for (int l = 0; l < n; ++l) {
+        const double kk = p->k[i] * p->k[i] + p->k[j] * p->k[j] + p->k[l] * p->k[l];
+        int s = (int)std::floor(std::sqrt(kk) / p->shell_w + 0.5);
+        p->counts[std::min(s, p->nbins - 1)]++;
+      }
+  p->max_tiles = std::max(tiles_of(p, AX_Z), tiles_of(p, AX_X));
+  return GPE_OK;
+}
+
+template <typename R>
+int upload_tables(gpe_plan* p, const gpe_desc* d) {
+  const int n = p->n;
+  // twiddles W_n^j = exp(-2 pi i j/n), computed in long double and rounded once
+  std::vector<typename Cx<R>::T> tw(n), twl(n);
+  for (int j = 0; j < n; ++j) {
+    const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)j / (long double)n;
+    const long double c = cosl(a), s = sinl(a);
+    tw[j].x = (R)(double)c;
+    tw[j].y = (R)(double)s;
+    // residuals: complex64 applies twiddles as hi + lo (exact value and modulus)
+    twl[j].x = sizeof(R) == 4 ? (R)(double)(c - (long double)tw[j].x) : (R)0;
+    twl[j].y = sizeof(R) == 4 ? (R)(double)(s - (long double)tw[j].y) : (R)0;
+  }
+  CU(cudaMalloc(&p->d_tw, 2 * n * sizeof(tw[0])));
+  CU(cudaMemcpy(p->d_tw, tw.data(), n * sizeof(tw[0]), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy((char*)p->d_tw + n * sizeof(tw[0]), twl.data(), n * sizeof(tw[0]), cudaMemcpyHostToDevice));
+  // static axis potentials
+  std::vector<R> vax(3 * n, (R)0);
+  const double* ap[] = {d->static_x, d->static_y, d->static_z};
+  const int al[] = {d->static_x_len, d->static_y_len, d->static_z_len};
+  for (int a = 0; a < 3; ++a) {
+    if (!al[a]) continue;
+    std::vector<double> prog(ap[a], ap[a] + al[a]);
+    for (int i = 0; i < n; ++i) {
+      const double c = p->x[i];
+      vax[a * n + i] = (R)host_eval(prog, a == 0 ? c : 0.0, a == 1 ? c : 0.0, a == 2 ? c : 0.0, 0.0);
+    }
+  }
+  CU(cudaMalloc(&p->d_vax, 3 * n * sizeof(R)));
+  CU(cudaMemcpy(p->d_vax, vax.data(), 3 * n * sizeof(R), cudaMemcpyHostToDevice));
+  return GPE_OK;
+}
+
+int build_static(gpe_plan* p, const void* v, int v_kind, cudaStream_t st) {
+  const size_t m = (size_t)p->n * p->n * p->n;
+  const size_t rs = p->dtype == GPE_C64 ? 4 : 8;
+  const bool need_re = !p->prog_static_g.empty() || v_kind != GPE_V_NONE;
+  const bool need_im = v_kind == GPE_V_CPLX128 && p->kind == GPE_REAL;
+  if (need_re && !p->d_vre) CU(cudaMalloc(&p->d_vre, m * rs));
+  if (need_im && !p->d_vim) CU(cudaMalloc(&p->d_vim, m * rs));
+  if (!need_re && p->d_vre) { CU(cudaFree(p->d_vre)); p->d_vre = nullptr; }
+  if (!need_im && p->d_vim) { CU(cudaFree(p->d_vim)); p->d_vim = nullptr; }
+  p->ph.vre = p->d_vre;
+  p->ph.vim = p->d_vim;
+  if (!need_re && !need_im) return GPE_OK;
+  const int len = (int)p->prog_static_g.size();
+  if (p->dtype == GPE_C64)
+    k_build_static<float><<<1184, 256, 0, st>>>(p->n, p->d_x, p->d_prog_g, len, v, v_kind,
+                                               (float*)p->d_vre, (float*)p->d_vim);
+  else
+    k_build_static<double><<<1184, 256, 0, st>>>(p->n, p->d_x, p->d_prog_g, len, v, v_kind,
+                                                (double*)p->d_vre, (double*)p->d_vim);
+  CU(cudaGetLastError());
+  return GPE_OK;
+}
+
+void free_plan(gpe_plan* p) {
+  for (auto& r : p->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  for (auto e : p->pool) cudaEventDestroy(e);
+  void* bufs[] = {p->d_x, p->d_k, p->d_kin, p->d_kth, p->d_vax, p->d_vre, p->d_vim, p->d_prog_g, p->d_dyn,
+                  p->d_tw, p->d_partial, p->d_ticket, p->d_scale, p->d_status, p->d_hist, p->d_out,
+                  p->d_work};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  delete p;
+}
+
+int create(const gpe_desc* d, gpe_plan** out) {
+  gpe_plan* p = new gpe_plan();
+  int rc = fill_plan(p, d);
+  if (rc != GPE_OK) { delete p; return rc; }
+  const int n = p->n;
+  CU(cudaMalloc(&p->d_x, n * sizeof(double)));
+  CU(cudaMemcpy(p->d_x, p->x.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  CU(cudaMalloc(&p->d_k, n * sizeof(double)));
+  CU(cudaMemcpy(p->d_k, p->k.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  // kinetic factors per axis: exp(-i ckin k^2 dt) or exp(-ckin k^2 dt)
+  std::vector<double2> kin(n);
+  for (int i = 0; i < n; ++i) {
+    const double ph = p->ckin * p->k[i] * p->k[i] * p->dt;
+    kin[i] = p->kind == GPE_IMAGINARY ? make_double2(std::exp(-ph), 0.0)
+                                      : make_double2(std::cos(ph), -std::sin(ph));
+  }
+  CU(cudaMalloc(&p->d_kin, n * sizeof(double2)));
+  CU(cudaMemcpy(p->d_kin, kin.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+  std::vector<double> kth(n);
+  for (int i = 0; i < n; ++i) kth[i] = p->ckin * p->k[i] * p->k[i] * p->dt;
+  CU(cudaMalloc(&p->d_kth, n * sizeof(double)));
+  CU(cudaMemcpy(p->d_kth, kth.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  rc = p->dtype == GPE_C64 ? upload_tables<float>(p, d) : upload_tables<double>(p, d);
+  if (rc != GPE_OK) { free_plan(p); return rc; }
+  if (!p->prog_static_g.empty()) {
+    CU(cudaMalloc(&p->d_prog_g, p->prog_static_g.size() * sizeof(double)));
+    CU(cudaMemcpy(p->d_prog_g, p->prog_static_g.data(), p->prog_static_g.size() * sizeof(double),
+                  cudaMemcpyHostToDevice));
+  }
+  if (!p->prog_dyn.empty()) {
+    CU(cudaMalloc(&p->d_dyn, p->prog_dyn.size() * sizeof(double)));
+    CU(cudaMemcpy(p->d_dyn, p->prog_dyn.data(), p->prog_dyn.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  CU(cudaMalloc(&p->d_partial, 2 * 4 * (size_t)p->max_tiles * sizeof(double)));
+  CU(cudaMalloc(&p->d_ticket, sizeof(unsigned)));
+  CU(cudaMemset(p->d_ticket, 0, sizeof(unsigned)));
+  CU(cudaMalloc(&p->d_scale, 4 * sizeof(double)));
+  const double one[4] = {1.0, 1.0, 1.0, 0.0};
+  CU(cudaMemcpy(p->d_scale, one, sizeof(one), cudaMemcpyHostToDevice));
+  CU(cudaMalloc(&p->d_status, sizeof(int)));
+  CU(cudaMemset(p->d_status, 0, sizeof(int)));
+  CU(cudaMalloc(&p->d_out, (4 + p->nbins) * sizeof(double)));
+  Phys& ph = p->ph;
+  ph.kind = p->kind;
+  ph.beta = p->beta;
+  ph.dt = p->dt;
+  ph.ckin = p->ckin;
+  ph.inv_m = 1.0 / ((double)n * n * n);
+  ph.dx3 = p->dx * p->dx * p->dx;
+  ph.x = p->d_x;
+  ph.k = p->d_k;
+  ph.kin = p->d_kin;
+  ph.kth = p->d_kth;
+  ph.vax = p->d_vax;
+  ph.dyn = p->d_dyn;
+  ph.dyn_len = (int)p->prog_dyn.size();
+  ph.beam = d->beam_enabled ? 1 : 0;
+  ph.beam_amp = d->beam_amp;
+  ph.beam_inv_w2 = d->beam_enabled ? 1.0 / (d->beam_width * d->beam_width) : 0.0;
+  ph.beam_radius = d->beam_radius;
+  ph.beam_omega = d->beam_omega;
+  ph.beam_t_ramp = d->beam_t_ramp;
+  ph.kcut = d->k_cut_enabled ? 1 : 0;
+  ph.kcut2 = d->k_cut * d->k_cut;
+  ph.local_fp64 = d->local_fp64 ? 1 : 0;
+  rc = build_static(p, nullptr, GPE_V_NONE, 0);
+  if (rc != GPE_OK) { free_plan(p); return rc; }
+  CU(cudaDeviceSynchronize());
+  *out = p;
+  return GPE_OK;
+}
+
+// One Strang step (5 sweeps) whose half-steps use time `t` (t_mid);
+// `scaled` = psi carries a pending renormalisation.
+int strang_step(gpe_plan* p, void* psi, double t, bool scaled, cudaStream_t st) {
+  const bool imag = p->kind == GPE_IMAGINARY;
+  Sweep s = mk_sweep(psi, psi);
+  s.pre = PW_HALF1 | (scaled ? PW_SCALE : 0u);
+  s.fft1 = 1;
+  s.t1 = t;
+  TRY(sweep(p, AX_Z, s, st));
+  s = mk_sweep(psi, psi);
+  s.fft1 = 1;
+  TRY(sweep(p, AX_Y, s, st));
+  s = mk_sweep(psi, psi);
+  s.fft1 = 1;
+  s.mid = PW_KIN | PW_CONJ_LAST;
+  s.fft2 = 1;
+  s.post = PW_CONJ_FIRST;
+  TRY(sweep(p, AX_X, s, st));
+  s = mk_sweep(psi, psi);
+  s.pre = PW_CONJ_LAST;
+  s.fft1 = 1;
+  s.post = PW_CONJ_FIRST;
+  TRY(sweep(p, AX_Y, s, st));
+  s = mk_sweep(psi, psi);
+  s.pre = PW_CONJ_LAST;
+  s.fft1 = 1;
+  s.post = PW_CONJ_FIRST | PW_INVM | PW_HALF1 | (imag ? PW_NORM : 0u);
+  s.t1 = t;
+  s.partial = p->d_partial;
+  TRY(sweep(p, AX_Z, s, st));
+  return GPE_OK;
+}
+
+int fft3d(gpe_plan* p, const void* in, void* out, bool inverse, cudaStream_t st) {
+  if (!inverse) {
+    Sweep s = mk_sweep(in, out);
+    s.fft1 = 1;
+    TRY(sweep(p, AX_Z, s, st));
+    s.src = out;
+    TRY(sweep(p, AX_Y, s, st));
+    TRY(sweep(p, AX_X, s, st));
+    return GPE_OK;
+  }
+  Sweep s = mk_sweep(in, out);
+  s.pre = PW_CONJ_LAST;
+  s.fft1 = 1;
+  s.post = PW_CONJ_FIRST;
+  TRY(sweep(p, AX_X, s, st));
+  s.src = out;
+  TRY(sweep(p, AX_Y, s, st));
+  s.post = PW_CONJ_FIRST | PW_INVM;
+  TRY(sweep(p, AX_Z, s, st));
+  return GPE_OK;
+}
+
+// k-space reductions of a spectrum `f` (no FFT): partial area B + histogram.
+int kspace_reduce(gpe_plan* p, const void* f, cudaStream_t st) {
+  TRY(ensure_hist(p));
+  Sweep s = mk_sweep(f, nullptr);
+  s.post = PW_DIAG_K;
+  s.partial = p->d_partial + 4 * (size_t)p->max_tiles;
+  s.hist = p->d_hist;
+  return sweep(p, AX_X, s, st);
+}
+
+int finish_diag(gpe_plan* p, int na, bool hist, std::vector<double>& host, cudaStream_t st) {
+  const int nb = tiles_of(p, AX_X);
+  k_finish_diag<<<1, 256, 0, st>>>(p->d_partial, na, p->d_partial + 4 * (size_t)p->max_tiles, nb,
+                                   hist ? p->d_hist : nullptr, p->nbins, p->d_out);
+  CU(cudaGetLastError());
+  host.assign(4 + p->nbins, 0.0);
+  CU(cudaMemcpyAsync(host.data(), p->d_out, host.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  return GPE_OK;
+}
+
+}  // namespace
+
+// ================================================================ C ABI
+extern "C" {
+
+int gpe_version(void) { return 1; }
+
+int gpe_last_error(char* buf, size_t len) {
+  if (!buf || !len) return (int)g_err.size();
+  snprintf(buf, len, "%s", g_err.c_str());
+  return (int)g_err.size();
+}
+
+int gpe_plan_create(const gpe_desc* desc, gpe_plan** plan) {
+  if (!desc || !plan) return fail(GPE_ERR_ARG, "null argument");
+  *plan = nullptr;
+  return create(desc, plan);
+}
+
+int gpe_plan_destroy(gpe_plan* plan) {
+  if (!plan) return GPE_OK;
+  free_plan(plan);
+  return GPE_OK;
+}
+
+int gpe_plan_info(const gpe_plan* p, int* n, int* dtype, int* kind, int* nk_bins) {
+  if (!p) return fail(GPE_ERR_ARG, "null plan");
+  if (n) *n = p->n;
+  if (dtype) *dtype = p->dtype;
+  if (kind) *kind = p->kind;
+  if (nk_bins) *nk_bins = p->nbins;
+  return GPE_OK;
+}
+
+int gpe_set_static_potential(gpe_plan* p, const void* v, int v_kind, void* stream) {
+  if (!p) return fail(GPE_ERR_ARG, "null plan");
+  if (v_kind != GPE_V_NONE && v_kind != GPE_V_REAL64 && v_kind != GPE_V_CPLX128)
+    return fail(GPE_ERR_ARG, "unknown static potential kind");
+  if (v_kind != GPE_V_NONE && !v) return fail(GPE_ERR_ARG, "null static potential");
+  if (v_kind == GPE_V_CPLX128 && p->kind == GPE_IMAGINARY)
+    return fail(GPE_ERR_ARG, "imaginary time takes a real (float64) static potential");
+  return build_static(p, v, v_kind, (cudaStream_t)stream);
+}
+
+int gpe_step(gpe_plan* p, void* psi, int nsteps, long long step0, void* stream) {
+  if (!p || !psi) return fail(GPE_ERR_ARG, "null argument");
+  if (nsteps < 0) return fail(GPE_ERR_ARG, "nsteps must be >= 0");
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool imag = p->kind == GPE_IMAGINARY;
+  for (int s = 0; s < nsteps; ++s) TRY(strang_step(p, psi, t_mid_host(p, step0 + s), imag && s > 0, st));
+  if (imag && nsteps > 0) TRY(scale_sweep(p, psi, st));
+  return GPE_OK;
+}
+
+int gpe_step_at(gpe_plan* p, void* psi, double t, void* stream) {
+  if (!p || !psi) return fail(GPE_ERR_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  // reference: t_mid = float(t) + dt/2 (gpe/make_propagator.py:94)
+  TRY(strang_step(p, psi, t + p->dt / 2, false, st));
+  if (p->kind == GPE_IMAGINARY) TRY(scale_sweep(p, psi, st));
+  return GPE_OK;
+}
+
+int gpe_halfstep(gpe_plan* p, void* psi, double t, void* stream) {
+  if (!p || !psi) return fail(GPE_ERR_ARG, "null argument");
+  Sweep s = mk_sweep(psi, psi);
+  s.pre = PW_HALF1;
+  s.t1 = t;
+  return sweep(p, AX_Z, s, (cudaStream_t)stream);
+}
+
+int gpe_fft3d(gpe_plan* p, const void* in, void* out, int inverse, void* stream) {
+  if (!p || !in || !out) return fail(GPE_ERR_ARG, "null argument");
+  return fft3d(p, in, out, inverse != 0, (cudaStream_t)stream);
+}
+
+int gpe_normalise(gpe_plan* p, void* psi, void* stream) {
+  if (!p || !psi) return fail(GPE_ERR_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  TRY(norm_sweep(p, psi, st));
+  return scale_sweep(p, psi, st);
+}
+
+int gpe_norm(gpe_plan* p, const void* psi, double* norm, void* stream) {
+  if (!p || !psi || !norm) return fail(GPE_ERR_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  TRY(norm_sweep(p, psi, st));
+  CU(cudaMemcpyAsync(norm, p->d_scale + 2, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  return GPE_OK;
+}
+
+int gpe_kinetic_energy(gpe_plan* p, const void* psi_k, double* e_kin, void* stream) {
+  if (!p || !psi_k || !e_kin) return fail(GPE_ERR_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  TRY(kspace_reduce(p, psi_k, st));
+  std::vector<double> h;
+  TRY(finish_diag(p, 0, false, h, st));
+  *e_kin = h[3] * p->ph.dx3 * p->ph.inv_m;
+  return GPE_OK;
+}
+
+int gpe_nk_extraction(gpe_plan* p, const void* psi_k, double* occupation, long long* counts, void* stream) {
+  if (!p || !psi_k) return fail(GPE_ERR_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  TRY(kspace_reduce(p, psi_k, st));
+  std::vector<double> h;
+  TRY(finish_diag(p, 0, true, h, st));
+  const double f = p->ph.dx3 * p->ph.inv_m;
+  if (occupation)
+    for (int b = 0; b < p->nbins; ++b) occupation[b] = h[4 + b] * f;
+  if (counts)
+    for (int b = 0; b < p->nbins; ++b) counts[b] = p->counts[b];
+  return GPE_OK;
+}
+
+int gpe_diagnostics(gpe_plan* p, const void* psi, double t, double* scalars, double* nk, long long* counts,
+                    void* stream) {
+  if (!p || !psi || !scalars) return fail(GPE_ERR_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  TRY(ensure_work(p));
+  TRY(ensure_hist(p));
+  Sweep s = mk_sweep(psi, p->d_work);
+  s.pre = PW_DIAG_R;
+  s.t1 = t;
+  s.fft1 = 1;
+  s.partial = p->d_partial;
+  TRY(sweep(p, AX_Z, s, st));
+  const int na = tiles_of(p, AX_Z);
+  s = mk_sweep(p->d_work, p->d_work);
+  s.fft1 = 1;
+  TRY(sweep(p, AX_Y, s, st));
+  s = mk_sweep(p->d_work, nullptr);
+  s.fft1 = 1;
+  s.post = PW_DIAG_K;
+  s.partial = p->d_partial + 4 * (size_t)p->max_tiles;
+  s.hist = p->d_hist;
+  TRY(sweep(p, AX_X, s, st));
+  std::vector<double> h;
+  TRY(finish_diag(p, na, nk != nullptr, h, st));
+  const double dx3 = p->ph.dx3;
+  const double N = h[0] * dx3;
+  const double e_kin = p->ckin * h[3] * dx3 * p->ph.inv_m;
+  const double e_pot = h[1] * dx3;
+  const double e_int = 0.5 * p->beta * h[2] * dx3;
+  scalars[0] = N;
+  scalars[1] = e_kin;
+  scalars[2] = e_pot;
+  scalars[3] = e_int;
+  scalars[4] = e_kin + e_pot + e_int;
+  scalars[5] = (e_kin + e_pot + 2.0 * e_int) / N;
+  if (nk)
+    for (int b = 0; b < p->nbins; ++b) nk[b] = h[4 + b] * dx3 * p->ph.inv_m;
+  if (counts)
+    for (int b = 0; b < p->nbins; ++b) counts[b] = p->counts[b];
+  return GPE_OK;
+}
+
+int gpe_launch_count(const gpe_plan* p, long long* count) {
+  if (!p || !count) return fail(GPE_ERR_ARG, "null argument");
+  *count = p->launches;
+  return GPE_OK;
+}
+
+int gpe_profile(gpe_plan* p, int enable) {
+  if (!p) return fail(GPE_ERR_ARG, "null plan");
+  CU(cudaDeviceSynchronize());
+  for (auto& r : p->recs) { p->pool.push_back(r.a); p->pool.push_back(r.b); }
+  p->recs.clear();
+  p->prof = enable != 0;
+  return GPE_OK;
+}
+
+int gpe_profile_read(gpe_plan* p, double* ms, long long* count) {
+  if (!p || !ms || !count) return fail(GPE_ERR_ARG, "null argument");
+  for (int a = 0; a < 3; ++a) { ms[a] = 0.0; count[a] = 0; }
+  for (auto& r : p->recs) {
+    CU(cudaEventSynchronize(r.b));
+    float t = 0.f;
+    CU(cudaEventElapsedTime(&t, r.a, r.b));
+    ms[r.ax] += t;
+    count[r.ax] += 1;
+  }
+  return GPE_OK;
+}
+
+int gpe_status(gpe_plan* p, int* flags, void* stream) {
+  if (!p || !flags) return fail(GPE_ERR_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  CU(cudaMemcpyAsync(flags, p->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemsetAsync(p->d_status, 0, sizeof(int), st));
+  CU(cudaStreamSynchronize(st));
+  return GPE_OK;
+}
+
+}  // extern "C"

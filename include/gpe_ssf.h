@@ -1,0 +1,166 @@
+/*
+ * gpe_ssf.h -- C ABI of the B200 split-step Fourier propagator.
+ *
+ * Plain C types only: device buffers are passed as `void*` device pointers,
+ * host buffers as typed host pointers, CUDA streams as `void*`
+ * (a cudaStream_t; NULL = legacy default stream).  Every entry point returns a
+ * status code (GPE_OK = 0); gpe_last_error() gives the message of the last
+ * failure on the calling host thread.  A plan is not thread-safe: use one plan
+ * per host thread.  All launch functions are asynchronous on `stream` unless
+ * stated otherwise.
+ *
+ * Arrays are cubes `[x][y][z]` in C order (z fastest), complex64
+ * (interleaved float re,im) or complex128 (interleaved double re,im), as in the
+ * reference (`gpe/make_propagator.py:23-36`).
+ *
+ * Reference interfaces replaced (paths within PoyntingZhang/GPE_simulator):
+ *   gpe_plan_create      make_real_propagator / make_imag_propagator
+ *                        (gpe/make_propagator.py:5-8,106-108) + kernel factories
+ *                        (gpe/make_kernel.py:4-136); potentials from
+ *                        gpe/expressions.py:9-30 (as bytecode, not CUDA text)
+ *   gpe_set_static_potential   stage.staticV (gpe/stage.py:56-62)
+ *   gpe_step             the returned closures time_independent_propagator
+ *                        (gpe/make_propagator.py:12-54), time_dependent_propagator
+ *                        (:57-103), standard_imaginary_step (:109-151), called
+ *                        nsteps times as gpe/launch.py:8-13 does
+ *   gpe_step_at          one call of time_dependent_propagator(stage, t)
+ *                        (gpe/make_propagator.py:57-103)
+ *   gpe_halfstep         static_real_halfstep / dynamic_real_halfstep /
+ *                        imag_static_real_halfstep (gpe/make_kernel.py:14-119)
+ *   gpe_fft3d            cp.fft.fftn / cp.fft.ifftn (gpe/make_propagator.py:50,52)
+ *   gpe_norm             get_N (gpe/helper.py:81-88)
+ *   gpe_normalise        normalise (gpe/helper.py:91-93)
+ *   gpe_kinetic_energy   get_E (gpe/helper.py:135-140)
+ *   gpe_nk_extraction    nk_extraction (gpe/nk_extraction.py:16-45)
+ *   gpe_diagnostics      save_outputs' scalar + n(k) path (gpe/save.py:31-57),
+ *                        fused, plus total energy and chemical potential
+ */
+#ifndef GPE_SSF_H
+#define GPE_SSF_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define GPE_OK              0
+#define GPE_ERR_ARG         1   /* bad argument (reference: AssertionError / TypeError) */
+#define GPE_ERR_UNSUPPORTED 2   /* grid size with a prime factor > 13, or too large */
+#define GPE_ERR_CUDA        3   /* CUDA runtime error */
+#define GPE_ERR_OOM         4   /* device allocation failed */
+#define GPE_ERR_NONFINITE   5   /* a reduction saw NaN/Inf or a zero norm */
+#define GPE_ERR_TIMEOUT     6   /* a bounded device wait ran out */
+
+#define GPE_C64   0
+#define GPE_C128  1
+#define GPE_IMAGINARY 0
+#define GPE_REAL      1
+
+/* static potential array kinds for gpe_set_static_potential */
+#define GPE_V_NONE     0
+#define GPE_V_REAL64   1   /* float64 real cube (imaginary-time staticV) */
+#define GPE_V_CPLX128  2   /* complex128 cube U - i Gamma (real-time staticV) */
+
+/* Potential-expression bytecode: a flat double array, opcodes as doubles.
+ * Stack machine evaluated in FP64 per grid point. */
+#define GPE_OP_CONST 1  /* followed by one double operand */
+#define GPE_OP_X     2
+#define GPE_OP_Y     3
+#define GPE_OP_Z     4
+#define GPE_OP_T     5
+#define GPE_OP_ADD   6
+#define GPE_OP_SUB   7
+#define GPE_OP_MUL   8
+#define GPE_OP_DIV   9
+#define GPE_OP_POW   10
+#define GPE_OP_NEG   11
+#define GPE_OP_SIN   13
+#define GPE_OP_COS   14
+#define GPE_OP_TAN   15
+#define GPE_OP_EXP   16
+#define GPE_OP_SQRT  17
+#define GPE_OP_TANH  18
+#define GPE_OP_ABS   19
+#define GPE_OP_LOG   20
+#define GPE_PROGRAM_MAX   2048  /* doubles */
+#define GPE_STACK_MAX     32
+
+typedef struct gpe_plan gpe_plan;
+
+typedef struct gpe_desc {
+    int n;                    /* grid points per axis (prime factors <= 13, 2 <= n <= 1024) */
+    int dtype;                /* GPE_C64 or GPE_C128 */
+    int kind;                 /* GPE_IMAGINARY or GPE_REAL */
+    double beta;              /* nonlinear coefficient (stage.beta) */
+    double dt;                /* time step (stage.dt) */
+    double kinetic_coeff;     /* 1.0 = reference convention exp(-i k^2 dt) */
+    const double* x_array;    /* host, n values (stage.x_array) */
+    const double* k_array;    /* host, n values (stage.k_array) */
+    /* static potential = vx(x) + vy(y) + vz(z) + vg(x,y,z); each program optional */
+    const double* static_x;  int static_x_len;
+    const double* static_y;  int static_y_len;
+    const double* static_z;  int static_z_len;
+    const double* static_g;  int static_g_len;
+    /* time-dependent potential V(x,y,z,t) (real time only), optional */
+    const double* dynamic_g; int dynamic_g_len;
+    /* momentum cutoff (real time only) */
+    int k_cut_enabled;        double k_cut;
+    /* built-in rotating Gaussian stirring beam (real time only):
+     * amp*exp(-((x-r cos th)^2+(y-r sin th)^2)/w^2),
+     * th(t) = omega*(m^2/(2 t_ramp) + t - m), m = min(t, t_ramp); FP64 angle */
+    int beam_enabled;
+    double beam_amp, beam_width, beam_radius, beam_omega, beam_t_ramp;
+    /* n(k) shells: 0 = reference binning (width 2pi/L), else number of uniform bins */
+    int nk_bins;
+    /* complex64 plans: 1 = evaluate and apply the local half-step factor in FP64
+     * (0 = FP32 phase evaluation); ignored for complex128 */
+    int local_fp64;
+} gpe_desc;
+
+/* library */
+int  gpe_version(void);
+int  gpe_last_error(char* buf, size_t len);
+
+/* plans */
+int  gpe_plan_create(const gpe_desc* desc, gpe_plan** plan);
+int  gpe_plan_destroy(gpe_plan* plan);
+int  gpe_plan_info(const gpe_plan* plan, int* n, int* dtype, int* kind, int* nk_bins);
+int  gpe_set_static_potential(gpe_plan* plan, const void* v, int v_kind, void* stream);
+
+/* propagation (in place on psi; device pointer) */
+/* nsteps Strang steps; step i (i = step0 .. step0+nsteps-1) evaluates time-dependent
+ * potentials at t_mid = i*dt + dt/2 (gpe/launch.py:10 + gpe/make_propagator.py:94) */
+int  gpe_step(gpe_plan* plan, void* psi, int nsteps, long long step0, void* stream);
+/* one Strang step at an arbitrary time t (the closure call propagator(stage, t)) */
+int  gpe_step_at(gpe_plan* plan, void* psi, double t, void* stream);
+int  gpe_halfstep(gpe_plan* plan, void* psi, double t, void* stream);
+int  gpe_fft3d(gpe_plan* plan, const void* in, void* out, int inverse, void* stream);
+int  gpe_normalise(gpe_plan* plan, void* psi, void* stream);
+
+/* reductions (synchronise `stream`, results on the host) */
+int  gpe_norm(gpe_plan* plan, const void* psi, double* norm, void* stream);
+int  gpe_kinetic_energy(gpe_plan* plan, const void* psi_k, double* e_kin, void* stream);
+int  gpe_nk_extraction(gpe_plan* plan, const void* psi_k, double* occupation,
+                       long long* counts, void* stream);
+/* scalars[6] = {N, E_kin, E_pot, E_int, E, mu}; nk (nullable) = Nk per shell
+ * (length nk_bins from gpe_plan_info), counts (nullable) = modes per shell */
+int  gpe_diagnostics(gpe_plan* plan, const void* psi, double t, double* scalars,
+                     double* nk, long long* counts, void* stream);
+
+/* accounting: kernel launches issued by this plan since creation */
+int  gpe_launch_count(const gpe_plan* plan, long long* count);
+/* per-launch timing: enable = 1 brackets every sweep launch with CUDA events on its
+ * stream (enable = 0 stops; both discard earlier records); read synchronises and
+ * returns total milliseconds and launches per sweep axis (ms[3], count[3]: z, y, x) */
+int  gpe_profile(gpe_plan* plan, int enable);
+int  gpe_profile_read(gpe_plan* plan, double* ms, long long* count);
+
+/* device status word: bit 0 non-finite norm, bit 1 timeout; read and clear (synchronises) */
+int  gpe_status(gpe_plan* plan, int* flags, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPE_SSF_H */

@@ -1,0 +1,143 @@
+"""CUDA path vs fixtures generated by running the reference itself.
+
+The fixtures (``tests/golden/*.npz``, made by ``tests/golden/make_golden.py``)
+hold the reference's own outputs (its propagator closures, kernel strings and
+diagnostics, with numpy.fft in place of cuFFT).  complex128 must match to the
+north-star tolerance 1e-12 (psi relative L2); complex64 to 1e-5.
+"""
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ssf
+from tests.golden import cases
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def load(name):
+    return np.load(GOLD / f"{name}.npz")
+
+
+def rel(a, b):
+    return ssf.rel_l2(a, b)
+
+
+def plan_for(c, kind, dtype, **kw):
+    from gpe_simulator_b200 import Plan
+    x, k = ssf.get_grids(c["n"], c["L"])
+    return Plan(c["n"], x, k, dtype=dtype, kind=kind, beta=c["beta"], dt=c["dt"],
+                static_expr=c["static_expr"], **kw), x, k
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.complex128, 1e-12), (torch.complex64, 1e-5)])
+def test_ground_state_64(cuda, dtype, tol):
+    c = cases.GROUND64
+    g = load("ground64")
+    plan, x, k = plan_for(c, "imaginary", dtype)
+    psi = torch.from_numpy(ssf.noisy_gaussian(x, seed=c["seed"])).to(dtype).cuda()
+    done = 0
+    sub = c["sub"]
+    for mark in c["checkpoints"]:
+        plan.step(psi, mark - done, done)
+        done = mark
+        got = psi.cpu().numpy()
+        err = rel(got[::sub, ::sub, ::sub], g[f"psi_sub_{mark}"])
+        assert err < tol, (mark, err)
+        # projections on seeded random fields touch every point (the subsample does not)
+        proj = g[f"proj_{mark}"]
+        perr = np.max(np.abs(cases.projections(got) - proj)) / np.max(np.abs(proj))
+        assert perr < 10 * tol, (mark, perr)
+        N = plan.norm(psi)
+        assert abs(N - g[f"N_{mark}"]) < (1e-13 if dtype == torch.complex128 else 1e-6)
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.complex128, 1e-12), (torch.complex64, 2e-5)])
+def test_stirred_32(cuda, dtype, tol):
+    from gpe_simulator_b200 import Plan
+    c = cases.STIR32
+    g = load("stir32")
+    imag, x, k = plan_for(c, "imaginary", dtype)
+    psi = torch.from_numpy(ssf.noisy_gaussian(x, seed=c["seed"])).to(dtype).cuda()
+    imag.step(psi, c["imag_steps"])
+    sub = c["sub"]
+    assert rel(psi.cpu().numpy()[::sub, ::sub, ::sub], g["psi_start"]) < tol
+    b = cases.stir_beam()
+    from gpe_simulator_b200 import Beam
+    real = Plan(c["n"], x, k, dtype=dtype, kind="real", beta=c["beta"], dt=c["dt"],
+                static_expr=c["static_expr"],
+                beam=Beam(b.amp, b.width, b.radius, b.omega, b.t_ramp))
+    done = 0
+    for mark in c["checkpoints"]:
+        real.step(psi, mark - done, done)
+        done = mark
+        err = rel(psi.cpu().numpy()[::sub, ::sub, ::sub], g[f"psi_sub_{mark}"])
+        assert err < tol, (mark, err)
+        assert abs(real.norm(psi) - g[f"N_{mark}"]) < (1e-12 if dtype == torch.complex128 else 1e-6)
+
+
+def test_stirred_32_expression_path(cuda):
+    """The same beam written as a dynamic expression (device bytecode)."""
+    from gpe_simulator_b200 import Plan
+    c = cases.STIR32
+    g = load("stir32")
+    imag, x, k = plan_for(c, "imaginary", torch.complex128)
+    psi = torch.from_numpy(ssf.noisy_gaussian(x, seed=c["seed"])).cuda()
+    imag.step(psi, c["imag_steps"])
+    real = Plan(c["n"], x, k, dtype=torch.complex128, kind="real", beta=c["beta"], dt=c["dt"],
+                static_expr=c["static_expr"], dynamic_expr=cases.stir_beam().expression())
+    real.step(psi, c["checkpoints"][0])
+    err = rel(psi.cpu().numpy()[::2, ::2, ::2], g[f"psi_sub_{c['checkpoints'][0]}"])
+    assert err < 1e-12, err
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.complex128, 1e-12), (torch.complex64, 1e-5)])
+def test_lossy_cutoff_16(cuda, dtype, tol):
+    from gpe_simulator_b200 import Plan
+    c = cases.LOSSY16
+    g = load("lossy16")
+    x, k = ssf.get_grids(c["n"], c["L"])
+    plan = Plan(c["n"], x, k, dtype=dtype, kind="real", beta=c["beta"], dt=c["dt"],
+                static_expr=c["static_expr"], dynamic_expr=c["dynamic_expr"], k_cut=c["k_cut"])
+    plan.set_static_potential(torch.from_numpy(cases.lossy_potential(x, c)).cuda())
+    psi = torch.from_numpy(ssf.noisy_gaussian(x, sigma=1.5, seed=c["seed"])).to(dtype).cuda()
+    plan.step(psi, c["steps"])
+    assert rel(psi.cpu().numpy(), g["psi"]) < tol
+    assert abs(plan.norm(psi) - float(g["N"])) < 1e-6
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.complex128, 1e-12), (torch.complex64, 1e-5)])
+def test_box_potential_24(cuda, dtype, tol):
+    from gpe_simulator_b200 import Plan
+    c = cases.BOX24
+    g = load("box24")
+    x, k = ssf.get_grids(c["n"], c["L"])
+    plan = Plan(c["n"], x, k, dtype=dtype, kind="imaginary", beta=c["beta"], dt=c["dt"],
+                static_expr=c["static_expr"])
+    plan.set_static_potential(torch.from_numpy(cases.box_potential(x, c)).cuda())
+    psi = torch.from_numpy(ssf.noisy_gaussian(x, sigma=2.0, seed=c["seed"])).to(dtype).cuda()
+    plan.step(psi, c["steps"])
+    assert rel(psi.cpu().numpy(), g["psi"]) < tol
+
+
+@pytest.mark.parametrize("n,L", cases.DIAG_SIZES)
+def test_diagnostics_match_reference(cuda, n, L):
+    from gpe_simulator_b200 import helper
+    from gpe_simulator_b200.nk_extraction import nk_extraction
+    g = load(f"diag_n{n}")
+    x, k = helper.get_grids(n, L)
+    psi = torch.from_numpy(cases.diag_state(n)).cuda()
+    assert helper.get_N(psi, x) == pytest.approx(float(g["N"]), rel=1e-13)
+    F = helper.fftn(psi, x)
+    assert helper.get_E(F, x, k) == pytest.approx(float(g["E_kin"]), rel=1e-12)
+    spec = nk_extraction(F, x, k)
+    np.testing.assert_array_equal(spec["counts"], g["nk_counts"])
+    np.testing.assert_allclose(spec["Nk"], g["nk_Nk"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(spec["nk"], g["nk_nk"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_array_equal(spec["edges"], g["nk_edges"])
+    np.testing.assert_array_equal(spec["k"], g["nk_k"])
+    np.testing.assert_array_equal(spec["complete_shells"], g["nk_complete_shells"])

@@ -1,0 +1,180 @@
+"""Host-side logic that needs no GPU: expressions, bytecode, shells, C-ABI symbols."""
+
+import ctypes
+import math
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import expr as oexpr
+from oracle import ssf
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "gpe_ssf.h"
+
+
+# ------------------------------------------------------------------ expressions
+def test_cuda_expression_matches_reference_rendering():
+    """Strings the reference's own tests pin (``tests/test_workflow.py:25-32``)."""
+    from gpe_simulator_b200.expressions import cuda_expression
+    assert cuda_expression("1/2*y**2") == "((1.0 / 2.0) * pow(y, 2.0))"
+    assert cuda_expression("abs(-x) + cos(t)", True) == "(fabs((-x)) + cos(t))"
+    assert cuda_expression("pi") == repr(np.pi)
+    with pytest.raises(ValueError):
+        cuda_expression("t*y")
+    with pytest.raises(ValueError):
+        cuda_expression("x; return 0")
+
+
+def run_program(prog, x, y, z, t=0.0):
+    """Python model of the device stack machine (same opcodes as include/gpe_ssf.h)."""
+    st = []
+    pc = 0
+    fn = {13: np.sin, 14: np.cos, 15: np.tan, 16: np.exp, 17: np.sqrt, 18: np.tanh, 19: np.abs, 20: np.log}
+    while pc < len(prog):
+        op = int(prog[pc]); pc += 1
+        if op == 1:
+            st.append(prog[pc]); pc += 1
+        elif op in (2, 3, 4, 5):
+            st.append({2: x, 3: y, 4: z, 5: t}[op])
+        elif op in (6, 7, 8, 9, 10):
+            b, a = st.pop(), st.pop()
+            ops = {6: lambda: a + b, 7: lambda: a - b, 8: lambda: a * b, 9: lambda: a / b,
+                   10: lambda: a ** b}
+            st.append(ops[op]())
+        elif op == 11:
+            st.append(-st.pop())
+        else:
+            st.append(fn[op](st.pop()))
+    assert len(st) == 1
+    return st[0]
+
+
+EXPRS = ["x**2+1.44*y**2+2.25*z**2", "x/2 + y**2/10 + abs(z)/5", "0.002*(x*x + y*y + z*z)",
+         "-(x-1)**2 + 3*sin(y)*cos(z) - exp(-x*x)", "sqrt(x*x+y*y) - tanh(z) + log(2+x)", "1/2", "pi*x"]
+
+
+@pytest.mark.parametrize("source", EXPRS)
+def test_bytecode_and_separable_split_evaluate_like_the_oracle(source):
+    from gpe_simulator_b200.expressions import compile_program, split_static
+    rng = np.random.default_rng(0)
+    x, y, z = rng.uniform(0.1, 2.0, 3)
+    want = oexpr.evaluate(source, x, y, z)
+    assert run_program(compile_program(source), x, y, z) == pytest.approx(want, rel=1e-14, abs=1e-14)
+    px, py, pz, pg = split_static(source)
+    parts = [run_program(px, x, 0, 0) if px else 0.0, run_program(py, 0, y, 0) if py else 0.0,
+             run_program(pz, 0, 0, z) if pz else 0.0, run_program(pg, x, y, z) if pg else 0.0]
+    assert sum(parts) == pytest.approx(want, rel=1e-13, abs=1e-13)
+
+
+def test_separable_trap_has_no_general_part():
+    from gpe_simulator_b200.expressions import split_static
+    px, py, pz, pg = split_static("x**2+1.44*y**2+2.25*z**2")
+    assert px and py and pz and not pg
+    assert split_static("x*y")[3]
+
+
+def test_time_dependent_bytecode():
+    from gpe_simulator_b200.expressions import compile_program
+    beam = ssf.Beam(20.0, 0.5, 2.0, 1.0, 0.05)
+    src = beam.expression()
+    for t in (0.0, 0.01, 0.07):
+        got = run_program(compile_program(src, time_dependent=True), 1.2, -0.3, 0.4, t)
+        assert got == pytest.approx(float(beam.value(1.2, -0.3, t)), rel=1e-13)
+
+
+def test_reference_cuda_text_round_trips():
+    from gpe_simulator_b200.expressions import cuda_expression, from_cuda_text
+    for source in EXPRS:
+        back = from_cuda_text(cuda_expression(source))
+        x, y, z = 0.7, -1.1, 0.3
+        assert oexpr.evaluate(back, x, y, z) == pytest.approx(oexpr.evaluate(source, x, y, z), rel=1e-15)
+
+
+# ------------------------------------------------------------------ n(k) geometry
+@pytest.mark.parametrize("n", [2, 7, 8, 18, 256, 512])
+def test_reference_shell_count(n):
+    from gpe_simulator_b200.nk_extraction import shell_geometry
+    nb, width = shell_geometry(n, 0.5)
+    assert nb == ssf.reference_nbins(n) and width == 0.5
+    assert ssf.reference_nbins(256) == 223 and ssf.reference_nbins(512) == 444
+
+
+def test_assemble_matches_oracle_dictionary():
+    from gpe_simulator_b200.nk_extraction import assemble
+    n, L = 8, 2 * np.pi
+    x, k = ssf.get_grids(n, L)
+    F = np.fft.fftn(np.random.default_rng(1).normal(size=(n, n, n)) + 0j)
+    want = ssf.nk_extraction(F, x, k)
+    got = assemble(want["Nk"], want["counts"], n, 1.0)
+    for key in want:
+        np.testing.assert_allclose(got[key], want[key])
+
+
+# ------------------------------------------------------------------ C ABI
+def declared_functions():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(gpe_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    from gpe_simulator_b200 import _lib, build
+    build.build()
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    names = declared_functions()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_desc_struct_layout_matches_header(tmp_path):
+    """Offsets of gpe_desc as compiled by gcc equal the ctypes Structure's."""
+    from gpe_simulator_b200 import _lib
+    fields = [f for f, _ in _lib.Desc._fields_]
+    src = tmp_path / "layout.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+    lines += [f'printf("%zu\\n", offsetof(gpe_desc, {f}));' for f in fields]
+    lines += ['printf("%zu\\n", sizeof(gpe_desc));', "return 0;}"]
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", str(src), "-o", str(exe)], check=True)
+    out = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [getattr(_lib.Desc, f).offset for f in fields] + [ctypes.sizeof(_lib.Desc)]
+    assert out == want
+
+
+def test_status_codes_map_to_reference_exceptions():
+    from gpe_simulator_b200 import _lib
+    _lib.load()
+    _lib.check(_lib.GPE_OK)
+    with pytest.raises(ValueError):
+        _lib.check(_lib.GPE_ERR_ARG)
+    with pytest.raises(MemoryError):
+        _lib.check(_lib.GPE_ERR_OOM)
+    with pytest.raises(_lib.GpeError):
+        _lib.check(_lib.GPE_ERR_CUDA)
+
+
+def test_plan_create_rejects_bad_descriptors_without_a_gpu():
+    """Argument validation runs before any device call."""
+    from gpe_simulator_b200 import _lib
+    lib = _lib.load()
+    d = _lib.Desc()
+    d.n = 17 * 19
+    h = ctypes.c_void_p()
+    assert lib.gpe_plan_create(ctypes.byref(d), ctypes.byref(h)) == _lib.GPE_ERR_UNSUPPORTED
+    assert "prime factor" in _lib.last_error()
+    d.n = 1
+    assert lib.gpe_plan_create(ctypes.byref(d), ctypes.byref(h)) == _lib.GPE_ERR_UNSUPPORTED
+    d.n, d.dtype = 16, 7
+    assert lib.gpe_plan_create(ctypes.byref(d), ctypes.byref(h)) == _lib.GPE_ERR_ARG
+    x = (ctypes.c_double * 16)(*np.linspace(-1, 1, 16))
+    d.dtype, d.kind, d.x_array, d.k_array = 0, 0, x, x
+    bad = (ctypes.c_double * 3)(2.0, 6.0, 6.0)  # x, ADD with one operand on the stack
+    d.static_g, d.static_g_len = bad, 3
+    assert lib.gpe_plan_create(ctypes.byref(d), ctypes.byref(h)) == _lib.GPE_ERR_ARG
+    assert "program" in _lib.last_error()
