@@ -37,6 +37,7 @@ class Desc(ctypes.Structure):
         ("beam_t_ramp", ctypes.c_double),
         ("nk_bins", ctypes.c_int),
         ("local_fp64", ctypes.c_int),
+        ("generic_only", ctypes.c_int),
     ]
 
 

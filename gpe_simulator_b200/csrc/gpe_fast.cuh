@@ -1,0 +1,573 @@
+// gpe_fast.cuh -- register-resident sweep kernels for N = 64, 128, 256 (sm_100a).
+//
+// A line of length N = N1*N2 is transformed in two register phases with one
+// shared-memory exchange between them (the "four-step" split):
+//   phase 1: thread n1 (< N1) holds x[n1 + N1*n2], n2 < N2, and computes
+//            Y[n1][k2] = DFT_N2(x[n1 + N1*.])[k2] * W_N^(n1*k2);
+//   exchange through shared memory;
+//   phase 2: thread k2 (< N2) holds Y[.][k2] and computes
+//            X[k2 + N2*k1] = DFT_N1(Y[.][k2])[k1].
+// Values come straight from HBM into phase-1 registers and leave from phase-2
+// registers, so an FFT costs one shared-memory round trip.  The output layout
+// (thread k2 holds k2 + N2*k1) is the input layout of the same algorithm with
+// N1 and N2 swapped, so an inverse transform can start from the forward's
+// registers with no exchange (the kinetic sweep: forward, kinetic phase,
+// inverse).  Inverses are conj(FFT(conj(x))).
+//
+// Tiles: Z = L consecutive z-lines (contiguous in memory; consecutive lanes
+// walk along the line), P = L adjacent lines of the y or x axis (consecutive
+// lanes walk across lines, 128-byte rows).  Pointwise work (renormalisation,
+// half-steps, 1/M, kinetic phase, norm partials) runs on the registers.
+#pragma once
+#include "gpe_kernels.cuh"
+
+namespace gpe {
+
+template <int N> struct Split;
+template <> struct Split<64>  { static constexpr int N1 = 8,  N2 = 8;  };
+template <> struct Split<128> { static constexpr int N1 = 8,  N2 = 16; };
+template <> struct Split<256> { static constexpr int N1 = 16, N2 = 16; };
+
+// Lines per tile and threads per block of the fast sweeps (elements per thread = L*N/T).
+template <int N, typename R> struct FastCfg {
+  static constexpr int L = sizeof(R) == 4 ? 16 : 8;  // 128-byte rows for P tiles
+  static constexpr int T = L * N / 16;               // 16 elements per thread
+};
+
+enum : int { FZ = 0, FY = 1, FX = 2 };
+
+// shared exchange buffer (complex elements) covering both split orders and tile kinds
+template <int N, typename R> __host__ __device__ constexpr int fast_exchange_elems() {
+  return FastCfg<N, R>::L * (N + (Split<N>::N1 > Split<N>::N2 ? Split<N>::N1 : Split<N>::N2));
+}
+
+// runtime options of a fast sweep (uniform per launch)
+struct FastOps {
+  int mode;         // FM_* (selects the kernel)
+  int inv1;         // FM_PLAIN: inverse transform
+  int invm;         // FM_PLAIN: multiply by 1/M
+  int scale;        // FM_Z1: apply the pending renormalisation
+  int norm;         // FM_Z2: norm partials and renormalisation scale
+};
+
+// per-tile table bytes (kx, kyz, kx2, kyz2, vz, c1, c2), rounded to 16
+template <int N, typename R> __host__ __device__ constexpr size_t fast_tables_bytes() {
+  return (((size_t)(N + FastCfg<N, R>::L) * (16 + 8) + (size_t)(N + 2 * FastCfg<N, R>::L) * sizeof(R)) + 15)
+         / 16 * 16;
+}
+
+// shared memory of a fast sweep (bytes)
+template <int N, typename R> __host__ __device__ constexpr size_t fast_smem_bytes() {
+  return (size_t)(2 * N) * sizeof(typename Cx<R>::T)
+         + (size_t)FastCfg<N, R>::L * (N + (Split<N>::N1 > Split<N>::N2 ? Split<N>::N1 : Split<N>::N2))
+               * sizeof(typename Cx<R>::T)
+         + 32 * 4 * 16                                          /* Acc reduction */
+         + fast_tables_bytes<N, R>()
+         + (Split<N>::N1 == Split<N>::N2 ? 0 : (size_t)(2 * N) * sizeof(typename Cx<R>::T));  /* t2 */
+}
+
+template <int N, int AX, typename R>
+struct FastTile {
+  static constexpr int L = FastCfg<N, R>::L;
+  long long base;    // global index of (line 0, element 0)
+  long long nstride; // stride along the transform axis
+  long long lstride; // stride between lines
+  int a0, b0;        // Z: first line g; Y: (x, z0); X: (y, z0)
+  __device__ __forceinline__ FastTile(int tile) {
+    if (AX == FZ) {
+      a0 = tile * L; b0 = 0;
+      base = (long long)a0 * N; nstride = 1; lstride = N;
+    } else {
+      constexpr int tpr = N / L;
+      const int row = tile / tpr, z0 = (tile % tpr) * L;
+      a0 = row; b0 = z0;
+      lstride = 1;
+      if (AX == FY) { base = (long long)row * N * N + z0; nstride = N; }
+      else { base = (long long)row * N + z0; nstride = (long long)N * N; }
+    }
+  }
+  __device__ __forceinline__ void coords(int l, int m, int& i, int& j, int& k) const {
+    if (AX == FZ) { const int g = a0 + l; i = g / N; j = g % N; k = m; }
+    else if (AX == FY) { i = a0; j = m; k = b0 + l; }
+    else { i = m; j = a0; k = b0 + l; }
+  }
+  __device__ __forceinline__ long long gidx(int l, int m) const { return base + l * lstride + (long long)m * nstride; }
+};
+
+// Slot s of thread t in a phase with `per` lanes per line: Z tiles walk along the
+// line (lane fastest), P tiles across lines (line fastest).
+template <int AX, int LL>
+__device__ __forceinline__ void slot(int gs, int per, int& l, int& lane) {
+  if (AX == FZ) { lane = gs % per; l = gs / per; }
+  else { l = gs % LL; lane = gs / LL; }
+}
+
+// One forward FFT of every line of the tile, A = lanes in phase 1 (values A-strided),
+// B = values per lane in phase 1.  In: v[s][b] = x[lane_s + A*b] of line l_s (phase-1
+// slots).  Out: v[s][a] = X[lane_s + B*a] (phase-2 slots with B lanes per line).
+template <int N, int A, int B, int AX, typename R, int S1, int S2>
+__device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[S1 * B], typename Cx<R>::T* ex,
+                                           const typename Cx<R>::T* tw, const typename Cx<R>::T* twl) {
+  // tw/twl: 2-D twiddle table of this split, tw[k2*A + lane] = W_N^(lane*k2) (hi, lo):
+  // consecutive lanes read consecutive entries (no bank conflicts in Z tiles)
+  using C = typename Cx<R>::T;
+  constexpr int L = FastCfg<N, R>::L;
+  constexpr int T = FastCfg<N, R>::T;
+  static_assert(S1 * B == S2 * A, "register count must match between phases");
+  // phase 1: DFT_B over the registers, twiddle W_N^(lane*k2)
+#pragma unroll
+  for (int s = 0; s < S1; ++s) {
+    int l, lane;
+    slot<AX, L>(threadIdx.x + s * T, A, l, lane);
+    C* x = v + s * B;
+    Dft<B>::run(x, tw, twl, N / B);
+#pragma unroll
+    for (int k2 = 1; k2 < B; ++k2) {
+      const int e = k2 * A + lane;
+      x[k2] = twmul(x[k2], tw[e], twl[e]);
+    }
+    // exchange layout: Z tiles [l][k2][A + 1] (odd pitch), P tiles [k2][lane][L]
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) {
+      const int idx = AX == FZ ? (l * B + k2) * (A + 1) + lane : (k2 * A + lane) * L + l;
+      ex[idx] = x[k2];
+    }
+  }
+  __syncthreads();
+  // phase 2: lane k2 (< B) gathers Y[.][k2], DFT_A
+#pragma unroll
+  for (int s = 0; s < S2; ++s) {
+    int l, k2;
+    slot<AX, L>(threadIdx.x + s * T, B, l, k2);
+    C* x = v + s * A;
+#pragma unroll
+    for (int n1 = 0; n1 < A; ++n1) {
+      const int idx = AX == FZ ? (l * B + k2) * (A + 1) + n1 : (k2 * A + n1) * L + l;
+      x[n1] = ex[idx];
+    }
+    Dft<A>::run(x, tw, twl, N / A);
+  }
+  __syncthreads();
+}
+
+template <typename R>
+__device__ __forceinline__ typename Cx<R>::T conj_(typename Cx<R>::T v) { return mk(v.x, -v.y); }
+
+template <int EPT, typename C>
+__device__ __forceinline__ void conj_all(C (&v)[EPT]) {
+#pragma unroll
+  for (int q = 0; q < EPT; ++q) v[q].y = -v[q].y;
+}
+
+template <int EPT, typename C, typename R>
+__device__ __forceinline__ void scale_all(C (&v)[EPT], R f) {
+#pragma unroll
+  for (int q = 0; q < EPT; ++q) { v[q].x *= f; v[q].y *= f; }
+}
+
+enum : int { FM_PLAIN = 0, FM_Z1 = 1, FM_Z2 = 2, FM_Z21 = 3, FM_XKIN = 4 };
+
+// sin(x) and cos(x) - 1 from their Taylor series (Horner, FP32), valid for
+// |x| <= pi/4 where the first omitted terms (x^13/13!, x^14/14!) are below 1e-11;
+// callers use sincosf for larger arguments.
+__device__ __forceinline__ void sin_cosm1_series(float x, float& s, float& cm1) {
+  {
+    const float z = x * x;
+    s = x * fmaf(z, fmaf(z, fmaf(z, fmaf(z, fmaf(z, -2.5052108385441720e-08f, 2.7557319223985888e-06f),
+                                         -1.9841269841269841e-04f), 8.3333333333333333e-03f),
+                         -1.6666666666666667e-01f), 1.0f);
+    cm1 = z * fmaf(z, fmaf(z, fmaf(z, fmaf(z, fmaf(z, 2.0876756987868099e-09f, -2.7557319223985891e-07f),
+                                           2.4801587301587302e-05f), -1.3888888888888889e-03f),
+                           4.1666666666666667e-02f), -0.5f);
+  }
+}
+
+// exp(x) - 1 from its Taylor series, valid for |x| <= 1/2 (first omitted term
+// x^10/10! < 3e-10); callers use expm1f beyond.
+__device__ __forceinline__ float expm1_series(float x) {
+  {
+    return x * fmaf(x, fmaf(x, fmaf(x, fmaf(x, fmaf(x, fmaf(x, fmaf(x, fmaf(x, 2.7557319223985891e-06f,
+           2.4801587301587302e-05f), 1.9841269841269841e-04f), 1.3888888888888889e-03f), 8.3333333333333333e-03f),
+           4.1666666666666667e-02f), 1.6666666666666667e-01f), 0.5f), 1.0f);
+  }
+}
+
+// Local half-step factor for a potential value V (reference gpe/make_kernel.py:14-119);
+// gam = Im V_static (real time, 0 if none).  complex64 applies v + v*(f - 1).
+template <typename R>
+__device__ __forceinline__ typename Cx<R>::T fast_local(const Phys& ph, typename Cx<R>::T v, R V, R gam) {
+  if (sizeof(R) == 8 || ph.local_fp64) {
+    const double vx = v.x, vy = v.y, hd = ph.dt * 0.5;
+    const double phd = ((double)V + ph.beta * (vx * vx + vy * vy)) * hd;
+    if (ph.kind == 0) {
+      const double f = exp(-phd);
+      return mk((R)(vx * f), (R)(vy * f));
+    }
+    double sd, cd;
+    sincos(phd, &sd, &cd);
+    if (gam != (R)0) {
+      const double a = exp((double)gam * hd);
+      cd *= a; sd *= a;
+    }
+    return mk((R)(vx * cd + vy * sd), (R)(vy * cd - vx * sd));
+  }
+  const float h = (float)(ph.dt * 0.5);
+  const float phase = ((float)V + (float)ph.beta * (v.x * v.x + v.y * v.y)) * h;
+  if (ph.kind == 0) {
+    const float e = fabsf(phase) <= 0.5f ? expm1_series(-phase) : expm1f(-phase);
+    return mk(fma(v.x, (R)e, v.x), fma(v.y, (R)e, v.y));
+  }
+  float cm1, sn;
+  if (fabsf(phase) <= 0.78539816f) {
+    sin_cosm1_series(phase, sn, cm1);
+  } else {
+    float sh, ch;
+    sincosf(0.5f * phase, &sh, &ch);
+    cm1 = -2.0f * sh * sh;
+    sn = 2.0f * sh * ch;
+  }
+  if (gam != (R)0) {
+    const float am1 = expm1f((float)gam * h);
+    cm1 = am1 + cm1 + am1 * cm1;
+    sn = sn + sn * am1;
+  }
+  return mk(fma(v.x, (R)cm1, fma(v.y, (R)sn, v.x)), fma(v.y, (R)cm1, fma(-v.x, (R)sn, v.y)));
+}
+
+// Per-tile tables in shared memory.
+template <typename R>
+struct FastTables {
+  R* vz;          // [N] static potential along z (Z tiles)
+  R* c1;          // [L] vx(i) + vy(j_l) + beam(i, j_l; t1)
+  R* c2;          // [L] same at t2
+  double2* kx;    // [N] kinetic factors along the transform axis (X tiles)
+  double2* kyz;   // [L] kinetic factor of (j, k_l)
+  double* kx2;    // [N] k^2 along x (cutoff)
+  double* kyz2;   // [L] k_j^2 + k_kl^2
+};
+
+template <int N, typename R>
+__device__ __forceinline__ void z_tables(const Phys& ph, const Sweep& sw, int a0, FastTables<R>& tb,
+                                         bool two) {
+  constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
+  const R* vax = (const R*)ph.vax;
+  for (int q = threadIdx.x; q < N; q += T) tb.vz[q] = vax[2 * N + q];
+  if (threadIdx.x < L) {
+    const int g = a0 + threadIdx.x, i = g / N, j = g % N;
+    const R base = vax[i] + vax[N + j];
+    R b1 = (R)0, b2 = (R)0;
+    if (ph.kind == 1 && ph.beam) {
+      // separable beam: amp * exp(-(x-cx)^2/w^2) * exp(-(y-cy)^2/w^2), centre from an FP64 angle
+      double cx, cy;
+      beam_centre(ph, sw.t1, cx, cy);
+      const R dx = (R)(ph.x[i] - cx), dy = (R)(ph.x[j] - cy), iw = (R)ph.beam_inv_w2;
+      b1 = (R)ph.beam_amp * rexp(-dx * dx * iw) * rexp(-dy * dy * iw);
+      if (two) {
+        beam_centre(ph, sw.t2, cx, cy);
+        const R ex = (R)(ph.x[i] - cx), ey = (R)(ph.x[j] - cy);
+        b2 = (R)ph.beam_amp * rexp(-ex * ex * iw) * rexp(-ey * ey * iw);
+      }
+    }
+    tb.c1[threadIdx.x] = base + b1;
+    tb.c2[threadIdx.x] = base + b2;
+  }
+}
+
+template <int N, typename R>
+__device__ __forceinline__ void x_tables(const Phys& ph, int j, int k0, FastTables<R>& tb) {
+  constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
+  for (int q = threadIdx.x; q < N; q += T) {
+    tb.kx[q] = ph.kin[q];
+    tb.kx2[q] = ph.k[q] * ph.k[q];
+  }
+  if (threadIdx.x < L) {
+    const int k = k0 + threadIdx.x;
+    const double2 a = ph.kin[j], b = ph.kin[k];
+    tb.kyz[threadIdx.x] = ph.kind == 0 ? make_double2(a.x * b.x, 0.0) : cmul(a, b);
+    tb.kyz2[threadIdx.x] = ph.k[j] * ph.k[j] + ph.k[k] * ph.k[k];
+  }
+}
+
+// Kinetic factor of (i, line l) applied in FP64 (reference gpe/kernels.py:3-66);
+// REAL / CUT are compile-time so the per-element code has no branches.
+template <typename R, bool REAL, bool CUT>
+__device__ __forceinline__ typename Cx<R>::T fast_kin(const Phys& ph, const FastTables<R>& tb,
+                                                      typename Cx<R>::T v, int i, int l) {
+  const double2 a = tb.kx[i], b = tb.kyz[l];
+  const double vx = v.x, vy = v.y;
+  typename Cx<R>::T out;
+  if (!REAL) {
+    const double f = a.x * b.x;
+    out = mk((R)(vx * f), (R)(vy * f));
+  } else {
+    const double fx = a.x * b.x - a.y * b.y, fy = a.x * b.y + a.y * b.x;
+    out = mk((R)(vx * fx - vy * fy), (R)(vx * fy + vy * fx));
+  }
+  if (CUT) {
+    const bool drop = tb.kx2[i] + tb.kyz2[l] > ph.kcut2;
+    out = drop ? mk((R)0, (R)0) : out;
+  }
+  return out;
+}
+
+template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT, bool REAL, bool CUT>
+__device__ __forceinline__ void kin_all(typename Cx<R>::T (&v)[EPT], const Phys& ph, const FastTables<R>& tb) {
+  constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
+#pragma unroll
+  for (int s = 0; s < SLOTS; ++s) {
+    int l, lane;
+    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+#pragma unroll
+    for (int a = 0; a < VALS; ++a) v[s * VALS + a] = fast_kin<R, REAL, CUT>(ph, tb, v[s * VALS + a], lane + LANES * a, l);
+  }
+}
+
+// One local half-step over all registers (layout LANES x VALS, element m = lane +
+// LANES*a, Z tiles: m = z index), potential vz[m] + ctab[l] (+ arrays).  The
+// phases are computed first; whether all of this thread's phases lie in the
+// series' range is decided once, so each element loop is straight-line code.
+template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT, bool REAL, bool ARR>
+__device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
+                                         const Phys& ph, const FastTables<R>& tb, const R* ctab,
+                                         R beta, R h) {
+  constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
+  R phs[EPT];
+  R gam[ARR ? EPT : 1];
+  bool small = true;
+#pragma unroll
+  for (int s = 0; s < SLOTS; ++s) {
+    int l, lane;
+    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+    const long long row = tl.base + (long long)l * tl.lstride;
+    const R c = ctab[l];
+#pragma unroll
+    for (int a = 0; a < VALS; ++a) {
+      const int e = s * VALS + a, m = lane + LANES * a;
+      R V = tb.vz[m] + c;
+      if (ARR) {
+        V += ph.vre ? ((const R*)ph.vre)[row + m] : (R)0;
+        gam[e] = ph.vim ? ((const R*)ph.vim)[row + m] * h : (R)0;
+      }
+      const typename Cx<R>::T x = v[e];
+      phs[e] = (V + beta * (x.x * x.x + x.y * x.y)) * h;
+      small = small && fabs(phs[e]) <= (REAL ? (R)0.78539816 : (R)0.5);
+    }
+  }
+  if (sizeof(R) == 8) {
+    // complex128: library exp / sincos in FP64 (the reference's arithmetic)
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      const typename Cx<R>::T x = v[e];
+      if (!REAL) {
+        const double f = exp(-(double)phs[e]);
+        v[e] = mk((R)(x.x * f), (R)(x.y * f));
+      } else {
+        double sd, cd;
+        sincos((double)phs[e], &sd, &cd);
+        if (ARR) { const double am = exp((double)gam[e]); sd *= am; cd *= am; }
+        v[e] = mk((R)(x.x * cd + x.y * sd), (R)(x.y * cd - x.x * sd));
+      }
+    }
+    return;
+  }
+  if (small) {
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      const typename Cx<R>::T x = v[e];
+      if (!REAL) {
+        const float em = expm1_series((float)-phs[e]);
+        v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
+      } else {
+        float sn, cm1;
+        sin_cosm1_series((float)phs[e], sn, cm1);
+        if (ARR) { const float am = expm1f((float)gam[e]); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
+        v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
+      }
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      const typename Cx<R>::T x = v[e];
+      if (!REAL) {
+        const float em = expm1f((float)-phs[e]);
+        v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
+      } else {
+        float sh, ch;
+        sincosf(0.5f * (float)phs[e], &sh, &ch);
+        float cm1 = -2.0f * sh * sh, sn = 2.0f * sh * ch;
+        if (ARR) { const float am = expm1f((float)gam[e]); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
+        v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
+      }
+    }
+  }
+}
+
+template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT>
+__device__ __forceinline__ void half_dispatch(typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
+                                              const Phys& ph, const FastTables<R>& tb, const R* ctab) {
+  const R beta = (R)ph.beta, h = (R)(ph.dt * 0.5);
+  const bool arr = ph.vre != nullptr || ph.vim != nullptr;
+  if (ph.kind == 1) {
+    if (arr) half_all<N, AX, R, LANES, VALS, SLOTS, EPT, true, true>(v, tl, ph, tb, ctab, beta, h);
+    else half_all<N, AX, R, LANES, VALS, SLOTS, EPT, true, false>(v, tl, ph, tb, ctab, beta, h);
+  } else {
+    if (arr) half_all<N, AX, R, LANES, VALS, SLOTS, EPT, false, true>(v, tl, ph, tb, ctab, beta, h);
+    else half_all<N, AX, R, LANES, VALS, SLOTS, EPT, false, false>(v, tl, ph, tb, ctab, beta, h);
+  }
+}
+
+// Pointwise stages of the fast modes on registers in layout (LANES lanes, VALS values).
+template <int N, int AX, typename R, int MODE, int STAGE, int LANES, int VALS, int SLOTS, int EPT>
+__device__ __forceinline__ void fast_pointwise(typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
+                                               const Phys& ph, const FastTables<R>& tb, const FastOps& op,
+                                               PwCtx<R>& cx) {
+  if (MODE == FM_XKIN) {
+    if (ph.kind == 1) {
+      if (ph.kcut) kin_all<N, AX, R, LANES, VALS, SLOTS, EPT, true, true>(v, ph, tb);
+      else kin_all<N, AX, R, LANES, VALS, SLOTS, EPT, true, false>(v, ph, tb);
+    } else {
+      kin_all<N, AX, R, LANES, VALS, SLOTS, EPT, false, false>(v, ph, tb);
+    }
+    return;
+  }
+  if (MODE == FM_Z1) {
+    if (op.scale) {
+      if (sizeof(R) == 8) {
+#pragma unroll
+        for (int e = 0; e < EPT; ++e) { v[e].x = (R)((double)v[e].x / cx.sc_div); v[e].y = (R)((double)v[e].y / cx.sc_div); }
+      } else {
+        scale_all(v, cx.sc_mul);
+      }
+    }
+    half_dispatch<N, AX, R, LANES, VALS, SLOTS, EPT>(v, tl, ph, tb, tb.c1);
+    return;
+  }
+  scale_all(v, (R)ph.inv_m);
+  half_dispatch<N, AX, R, LANES, VALS, SLOTS, EPT>(v, tl, ph, tb, tb.c1);
+  if (MODE == FM_Z21) half_dispatch<N, AX, R, LANES, VALS, SLOTS, EPT>(v, tl, ph, tb, tb.c2);
+  if (MODE == FM_Z2 && op.norm) {
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) cx.acc[0].add((double)v[e].x * v[e].x + (double)v[e].y * v[e].y);
+  }
+}
+
+// Load the tile into registers in layout (N1 lanes, N2 values).
+template <int N, int AX, typename R, int S1, int EPT>
+__device__ __forceinline__ void fast_load(typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
+                                          const typename Cx<R>::T* __restrict__ src, bool conj) {
+  constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+#pragma unroll
+  for (int s = 0; s < S1; ++s) {
+    int l, lane;
+    slot<AX, L>(threadIdx.x + s * T, N1, l, lane);
+#pragma unroll
+    for (int b = 0; b < N2; ++b) {
+      const typename Cx<R>::T x = src[tl.gidx(l, lane + N1 * b)];
+      v[s * N2 + b] = conj ? conj_<R>(x) : x;
+    }
+  }
+}
+
+template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT>
+__device__ __forceinline__ void fast_store(const typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
+                                           typename Cx<R>::T* __restrict__ dst) {
+  constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
+#pragma unroll
+  for (int s = 0; s < SLOTS; ++s) {
+    int l, lane;
+    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+#pragma unroll
+    for (int a = 0; a < VALS; ++a) dst[tl.gidx(l, lane + LANES * a)] = v[s * VALS + a];
+  }
+}
+
+// The sweep kernel of one mode.  Register layout before FFT #1: S1 slots of
+// (N1 lanes, N2 values); after FFT #1: S2 slots of (N2 lanes, N1 values) =
+// input layout of FFT #2 with (A, B) = (N2, N1); after FFT #2 the layout is
+// back to (N1 lanes, N2 values).
+//   FM_PLAIN  FFT (inverse if op.inv1; times 1/M if op.invm)       y sweeps, fftn/ifftn
+//   FM_Z1     [scale] half(t1), forward                             first z sweep of a step
+//   FM_Z2     inverse, 1/M, half(t1) [norm partials]                last z sweep of a step
+//   FM_Z21    inverse, 1/M, half(t1), half(t2), forward             last z of a step + first z of the next
+//   FM_XKIN   forward, kinetic, inverse                             x sweep
+template <int N, int AX, typename R, int MODE>
+__global__ void __launch_bounds__(FastCfg<N, R>::T) k_fast(Phys ph, Sweep sw, FastOps op) {
+  using C = typename Cx<R>::T;
+  constexpr int L = FastCfg<N, R>::L;
+  constexpr int T = FastCfg<N, R>::T;
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  constexpr int EPT = L * N / T;
+  constexpr int S1 = EPT / N2;
+  constexpr int S2 = EPT / N1;
+  constexpr bool ZM = MODE == FM_Z1 || MODE == FM_Z2 || MODE == FM_Z21;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = (C*)smem_raw;
+  C* twl = tw + N;
+  C* ex = twl + N;
+  Acc* red = (Acc*)(ex + fast_exchange_elems<N, R>());
+  unsigned char* tail = (unsigned char*)(red + 32 * 4);
+  FastTables<R> tb;
+  tb.kx = (double2*)tail;
+  tb.kyz = tb.kx + N;
+  tb.kx2 = (double*)(tb.kyz + L);
+  tb.kyz2 = tb.kx2 + N;
+  tb.vz = (R*)(tb.kyz2 + L);
+  tb.c1 = tb.vz + N;
+  tb.c2 = tb.c1 + L;
+  // 2-D twiddle tables: t1 for the split (N1 lanes, N2 values), t2 for (N2, N1)
+  C* t1 = tw;
+  C* t1l = twl;
+  C* t2 = (N1 == N2) ? t1 : (C*)(tail + fast_tables_bytes<N, R>());
+  C* t2l = (N1 == N2) ? t1l : t2 + N;
+  {
+    const C* g = (const C*)sw.tw;
+    const C* gl = (const C*)sw.tw_lo;
+    for (int q = threadIdx.x; q < N; q += T) {
+      const int k2 = q / N1, n1 = q % N1;   // t1[k2*N1 + n1] = W^(n1*k2)
+      t1[q] = g[(n1 * k2) & (N - 1)];
+      t1l[q] = gl[(n1 * k2) & (N - 1)];
+      if (N1 != N2) {
+        const int k2b = q / N2, n2 = q % N2;  // t2[k1*N2 + n2] = W^(n2*k1)
+        t2[q] = g[(n2 * k2b) & (N - 1)];
+        t2l[q] = gl[(n2 * k2b) & (N - 1)];
+      }
+    }
+  }
+  const FastTile<N, AX, R> tl(blockIdx.x);
+  if (ZM) z_tables<N, R>(ph, sw, tl.a0, tb, MODE == FM_Z21);
+  if (MODE == FM_XKIN) x_tables<N, R>(ph, tl.a0, tl.b0, tb);
+  PwCtx<R> cx;
+  cx.sc_div = 1.0;
+  cx.sc_mul = (R)1;
+  if (MODE == FM_Z1 && op.scale) {
+    cx.sc_div = __ldcg(sw.scale);
+    cx.sc_mul = (R)__ldcg(sw.scale + 1);
+  }
+
+  C v[EPT];
+  fast_load<N, AX, R, S1>(v, tl, (const C*)sw.src, MODE == FM_Z2 || MODE == FM_Z21 || (MODE == FM_PLAIN && op.inv1));
+  __syncthreads();  // twiddles and tables visible
+  if (MODE == FM_Z1) fast_pointwise<N, AX, R, MODE, 0, N1, N2, S1>(v, tl, ph, tb, op, cx);
+  fft_2phase<N, N1, N2, AX, R, S1, S2>(v, ex, t1, t1l);
+  if (MODE == FM_Z21 || MODE == FM_XKIN) {
+    if (MODE == FM_Z21) conj_all(v);  // finish the inverse before the physics
+    fast_pointwise<N, AX, R, MODE, 1, N2, N1, S2>(v, tl, ph, tb, op, cx);
+    if (MODE == FM_XKIN) conj_all(v);  // start the inverse
+    fft_2phase<N, N2, N1, AX, R, S2, S1>(v, ex, t2, t2l);
+    if (MODE == FM_XKIN) conj_all(v);
+    fast_store<N, AX, R, N1, N2, S1>(v, tl, (C*)sw.dst);
+  } else {
+    if (MODE == FM_Z2 || (MODE == FM_PLAIN && op.inv1)) conj_all(v);
+    if (MODE == FM_Z2) fast_pointwise<N, AX, R, MODE, 2, N2, N1, S2>(v, tl, ph, tb, op, cx);
+    if (MODE == FM_PLAIN && op.invm) scale_all(v, (R)ph.inv_m);
+    fast_store<N, AX, R, N2, N1, S2>(v, tl, (C*)sw.dst);
+  }
+  if (MODE == FM_Z2 && op.norm) {
+    Acc a[1] = {cx.acc[0]};
+    block_merge<1>(a, red);
+    norm_finish(ph, sw, a[0], red);
+  }
+}
+
+}  // namespace gpe

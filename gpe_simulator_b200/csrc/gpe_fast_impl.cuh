@@ -1,0 +1,51 @@
+// gpe_fast_impl.cuh -- launch wrappers of the register-resident sweeps for one precision.
+#pragma once
+#include "gpe_fast.cuh"
+#include "gpe_sweep.h"
+
+namespace gpe {
+
+template <int N, int AX, typename R, int MODE>
+static cudaError_t launch_fast_one(const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st) {
+  constexpr int L = FastCfg<N, R>::L;
+  constexpr int T = FastCfg<N, R>::T;
+  const int tiles = AX == FZ ? N * N / L : N * (N / L);
+  constexpr size_t smem = fast_smem_bytes<N, R>();
+  static int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaError_t e = cudaFuncSetAttribute(k_fast<N, AX, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_dev = dev;
+  }
+  k_fast<N, AX, R, MODE><<<tiles, T, smem, st>>>(ph, sw, op);
+  return cudaGetLastError();
+}
+
+template <int N, typename R>
+static cudaError_t launch_fast_n(int ax, const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st) {
+  switch (op.mode) {
+    case FM_Z1: return launch_fast_one<N, FZ, R, FM_Z1>(ph, sw, op, st);
+    case FM_Z2: return launch_fast_one<N, FZ, R, FM_Z2>(ph, sw, op, st);
+    case FM_Z21: return launch_fast_one<N, FZ, R, FM_Z21>(ph, sw, op, st);
+    case FM_XKIN: return launch_fast_one<N, FX, R, FM_XKIN>(ph, sw, op, st);
+    default: break;
+  }
+  if (ax == FZ) return launch_fast_one<N, FZ, R, FM_PLAIN>(ph, sw, op, st);
+  if (ax == FY) return launch_fast_one<N, FY, R, FM_PLAIN>(ph, sw, op, st);
+  return launch_fast_one<N, FX, R, FM_PLAIN>(ph, sw, op, st);
+}
+
+template <typename R>
+cudaError_t launch_fast(int n, int ax, const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st) {
+  switch (n) {
+    case 64: return launch_fast_n<64, R>(ax, ph, sw, op, st);
+    case 128: return launch_fast_n<128, R>(ax, ph, sw, op, st);
+    case 256: return launch_fast_n<256, R>(ax, ph, sw, op, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace gpe

@@ -1,6 +1,12 @@
 // gpe_ssf.cu -- plans, launch sequences and the C ABI (include/gpe_ssf.h).
 #include "../../include/gpe_ssf.h"
 #include "gpe_sweep.h"
+#include "gpe_fast.cuh"
+
+namespace gpe {
+template <typename R>
+cudaError_t launch_fast(int n, int ax, const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st);
+}
 
 #include <cmath>
 #include <cstdio>
@@ -175,6 +181,7 @@ struct gpe_plan {
   Phys ph{};
   int lt_z = 1, lt_yx = 16;
   bool gen = false;                // grid size needs the odd-prime radices 7/11/13
+  bool fast = false;               // register-resident sweeps exist for this n (64, 128, 256)
   int ept = 16;                    // elements per thread of the sweep family
   int nbins = 0;
   double shell_w = 0;
@@ -271,6 +278,38 @@ int sweep(gpe_plan* p, int ax, const Sweep& sw, cudaStream_t st) {
   return rc;
 }
 
+// Register-resident sweep (n in {64, 128, 256}); same accounting as sweep().
+int fsweep(gpe_plan* p, int ax, Sweep sw, const FastOps& op, cudaStream_t st) {
+  sw.pp = p->pp;
+  sw.tw = p->d_tw;
+  sw.tw_lo = (const char*)p->d_tw + (size_t)p->n * p->csize;
+  sw.ticket = p->d_ticket;
+  sw.scale = p->d_scale;
+  sw.status = p->d_status;
+  gpe_plan::Rec r{ax, nullptr, nullptr};
+  if (p->prof) {
+    r.a = pooled_event(p);
+    r.b = pooled_event(p);
+    CU(cudaEventRecord(r.a, st));
+  }
+  const int fax = ax == AX_Z ? FZ : ax == AX_Y ? FY : FX;
+  const cudaError_t e = p->dtype == GPE_C64 ? launch_fast<float>(p->n, fax, p->ph, sw, op, st)
+                                            : launch_fast<double>(p->n, fax, p->ph, sw, op, st);
+  if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("fast sweep: ") + cudaGetErrorString(e));
+  ++p->launches;
+  if (p->prof) {
+    CU(cudaEventRecord(r.b, st));
+    p->recs.push_back(r);
+  }
+  return GPE_OK;
+}
+
+FastOps mk_ops(int mode, int inv1 = 0, int invm = 0, int scale = 0, int norm = 0) {
+  FastOps o;
+  o.mode = mode; o.inv1 = inv1; o.invm = invm; o.scale = scale; o.norm = norm;
+  return o;
+}
+
 Sweep mk_sweep(const void* src, void* dst) {
   Sweep s;
   memset(&s, 0, sizeof(s));
@@ -345,6 +384,8 @@ int fill_plan(gpe_plan* p, const gpe_desc* d) {
   for (int q = 0; q < p->pp.npass; ++q)
     if (p->pp.radix[q] > 5 && p->pp.radix[q] != 8 && p->pp.radix[q] != 16) p->gen = true;
   p->ept = p->gen ? 8 : 16;
+  // register-resident sweeps: n = 64, 128, 256; potentials from tables (no per-point program)
+  p->fast = (n == 64 || n == 128 || n == 256) && !d->generic_only && d->dynamic_g_len == 0;
   const int emax = 512 * p->ept;
   p->lt_yx = std::max(1, std::min(d->dtype == GPE_C64 ? 16 : 8, emax / n));
   p->lt_z = std::max(1, std::min(n * n, std::min(4096, emax) / n));
@@ -543,7 +584,46 @@ int strang_step(gpe_plan* p, void* psi, double t, bool scaled, cudaStream_t st) 
   return GPE_OK;
 }
 
+// Fast path, 5 sweeps: Z(half, fwd) Y(fwd) X(fwd, kin, inv) Y(inv) Z(inv, 1/M, half [, norm]).
+// With `fuse_next`, the last sweep also applies the next step's half-step and
+// forward z transform (real time), so the next step starts at its Y sweep.
+int fast_front(gpe_plan* p, void* psi, double t, bool scaled, cudaStream_t st) {
+  Sweep s = mk_sweep(psi, psi);
+  s.t1 = t;
+  return fsweep(p, AX_Z, s, mk_ops(FM_Z1, 0, 0, scaled ? 1 : 0), st);
+}
+
+int fast_middle(gpe_plan* p, void* psi, cudaStream_t st) {
+  Sweep s = mk_sweep(psi, psi);
+  TRY(fsweep(p, AX_Y, s, mk_ops(FM_PLAIN), st));
+  TRY(fsweep(p, AX_X, s, mk_ops(FM_XKIN), st));
+  return fsweep(p, AX_Y, s, mk_ops(FM_PLAIN, 1), st);
+}
+
+int fast_back(gpe_plan* p, void* psi, double t, double t_next, bool fuse_next, cudaStream_t st) {
+  const bool imag = p->kind == GPE_IMAGINARY;
+  Sweep s = mk_sweep(psi, psi);
+  s.t1 = t;
+  s.t2 = t_next;
+  s.partial = p->d_partial;
+  if (fuse_next) return fsweep(p, AX_Z, s, mk_ops(FM_Z21), st);
+  return fsweep(p, AX_Z, s, mk_ops(FM_Z2, 0, 0, 0, imag ? 1 : 0), st);
+}
+
 int fft3d(gpe_plan* p, const void* in, void* out, bool inverse, cudaStream_t st) {
+  if (p->fast) {
+    Sweep s = mk_sweep(in, out);
+    if (!inverse) {
+      TRY(fsweep(p, AX_Z, s, mk_ops(FM_PLAIN), st));
+      s.src = out;
+      TRY(fsweep(p, AX_Y, s, mk_ops(FM_PLAIN), st));
+      return fsweep(p, AX_X, s, mk_ops(FM_PLAIN), st);
+    }
+    TRY(fsweep(p, AX_X, s, mk_ops(FM_PLAIN, 1), st));
+    s.src = out;
+    TRY(fsweep(p, AX_Y, s, mk_ops(FM_PLAIN, 1), st));
+    return fsweep(p, AX_Z, s, mk_ops(FM_PLAIN, 1, 1), st);
+  }
   if (!inverse) {
     Sweep s = mk_sweep(in, out);
     s.fft1 = 1;
@@ -635,6 +715,19 @@ int gpe_step(gpe_plan* p, void* psi, int nsteps, long long step0, void* stream) 
   if (nsteps < 0) return fail(GPE_ERR_ARG, "nsteps must be >= 0");
   cudaStream_t st = (cudaStream_t)stream;
   const bool imag = p->kind == GPE_IMAGINARY;
+  if (p->fast && nsteps > 0) {
+    // real time fuses each step's last z sweep with the next step's first
+    TRY(fast_front(p, psi, t_mid_host(p, step0), false, st));
+    for (int s = 0; s < nsteps; ++s) {
+      const double t = t_mid_host(p, step0 + s);
+      TRY(fast_middle(p, psi, st));
+      const bool fuse = !imag && s + 1 < nsteps;
+      TRY(fast_back(p, psi, t, t_mid_host(p, step0 + s + 1), fuse, st));
+      if (imag && s + 1 < nsteps) TRY(fast_front(p, psi, t_mid_host(p, step0 + s + 1), true, st));
+    }
+    if (imag) TRY(scale_sweep(p, psi, st));
+    return GPE_OK;
+  }
   for (int s = 0; s < nsteps; ++s) TRY(strang_step(p, psi, t_mid_host(p, step0 + s), imag && s > 0, st));
   if (imag && nsteps > 0) TRY(scale_sweep(p, psi, st));
   return GPE_OK;
@@ -644,7 +737,14 @@ int gpe_step_at(gpe_plan* p, void* psi, double t, void* stream) {
   if (!p || !psi) return fail(GPE_ERR_ARG, "null argument");
   cudaStream_t st = (cudaStream_t)stream;
   // reference: t_mid = float(t) + dt/2 (gpe/make_propagator.py:94)
-  TRY(strang_step(p, psi, t + p->dt / 2, false, st));
+  const double tm = t + p->dt / 2;
+  if (p->fast) {
+    TRY(fast_front(p, psi, tm, false, st));
+    TRY(fast_middle(p, psi, st));
+    TRY(fast_back(p, psi, tm, tm, false, st));
+  } else {
+    TRY(strang_step(p, psi, tm, false, st));
+  }
   if (p->kind == GPE_IMAGINARY) TRY(scale_sweep(p, psi, st));
   return GPE_OK;
 }

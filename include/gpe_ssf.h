@@ -117,6 +117,9 @@ typedef struct gpe_desc {
     /* complex64 plans: 1 = evaluate and apply the local half-step factor in FP64
      * (0 = FP32 phase evaluation); ignored for complex128 */
     int local_fp64;
+    /* 1 = use the generic mixed-radix sweeps even where register-resident sweeps
+     * exist (n = 64, 128, 256); for testing one path against the other */
+    int generic_only;
 } gpe_desc;
 
 /* library */

@@ -1,0 +1,68 @@
+"""The register-resident sweeps (n = 64, 128, 256) against the generic
+mixed-radix sweeps and the oracle, for every step sequence they implement."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ssf
+from tests.golden import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def make(n, L, kind, dtype, generic, **kw):
+    from gpe_simulator_b200 import Plan
+    x, k = ssf.get_grids(n, L)
+    return Plan(n, x, k, dtype=dtype, kind=kind, generic_only=generic, **kw), x
+
+
+@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("dtype,tol", [(torch.complex128, 1e-13), (torch.complex64, 3e-6)])
+@pytest.mark.parametrize("kind", ["imaginary", "real"])
+def test_fast_matches_generic_and_oracle(cuda, n, dtype, tol, kind):
+    from gpe_simulator_b200 import Beam
+    kw = dict(beta=800.0, dt=4e-4, static_expr=cases.TRAP)
+    if kind == "real":
+        kw["beam"] = Beam(20.0, 0.5, 2.0, 1.0, 0.004)
+    fast, x = make(n, 12.0, kind, dtype, False, **kw)
+    slow, _ = make(n, 12.0, kind, dtype, True, **kw)
+    psi0 = ssf.noisy_gaussian(x, seed=n)
+    a = torch.from_numpy(psi0).to(dtype).cuda()
+    b = a.clone()
+    fast.step(a, 7, 3)
+    slow.step(b, 7, 3)
+    err = ssf.rel_l2(a.cpu().numpy(), b.cpu().numpy())
+    assert err < tol, err
+    m = ssf.Model(n=n, simulation_range=12.0, kind=kind, beta=800.0, dt=4e-4, static_expr=cases.TRAP,
+                  beam=ssf.Beam(20.0, 0.5, 2.0, 1.0, 0.004) if kind == "real" else None)
+    want = ssf.run(psi0, m, 7, step0=3)
+    err = ssf.rel_l2(a.cpu().numpy(), want)
+    assert err < (1e-12 if dtype == torch.complex128 else 1e-5), err
+
+
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_fast_fft_matches_numpy(cuda, n):
+    p, _ = make(n, 10.0, "imaginary", torch.complex64, False, beta=0.0, dt=0.0)
+    g = torch.Generator(device="cuda").manual_seed(n)
+    a = torch.randn((n, n, n), dtype=torch.complex64, device="cuda", generator=g)
+    f = p.fft(a)
+    ref = torch.fft.fftn(a.to(torch.complex128))
+    err = ((f.to(torch.complex128) - ref).abs().pow(2).sum() / ref.abs().pow(2).sum()).sqrt().item()
+    assert err < 2e-6, err
+    back = p.fft(f, inverse=True)
+    err = ((back - a).abs().pow(2).sum() / a.abs().pow(2).sum()).sqrt().item()
+    assert err < 2e-6, err
+
+
+def test_step_at_equals_step(cuda):
+    """``propagator(stage, t)`` one call at a time equals one multi-step call."""
+    from gpe_simulator_b200 import Beam
+    p, x = make(64, 12.0, "real", torch.complex128, False, beta=500.0, dt=5e-4,
+                static_expr=cases.TRAP, beam=Beam(20.0, 0.5, 2.0, 1.0, 0.002))
+    a = torch.from_numpy(ssf.noisy_gaussian(x, seed=1)).cuda()
+    b = a.clone()
+    p.step(a, 6, 0)
+    for i in range(6):
+        p.step_at(b, i * 5e-4)
+    assert ssf.rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-14
