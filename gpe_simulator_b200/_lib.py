@@ -63,6 +63,7 @@ SIGNATURES = {
     "gpe_launch_count": [_vp, _llp],
     "gpe_profile": [_vp, ctypes.c_int],
     "gpe_profile_read": [_vp, _dp, _llp],
+    "gpe_normalise_noalloc": [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _vp],
 }
 
 _lib = None

@@ -18,7 +18,8 @@ INCLUDE = PKG.parent / "include"
 LIB = PKG / "libgpe_ssf.so"
 OBJ = PKG / "_build"
 
-SOURCES = ["gpe_ssf.cu", "gpe_sweep_f32.cu", "gpe_sweep_f64.cu", "gpe_fast_f32.cu", "gpe_fast_f64.cu"]
+SOURCES = ["gpe_ssf.cu", "gpe_sweep_f32.cu", "gpe_sweep_f64.cu", "gpe_fast_f32.cu", "gpe_fast_f64.cu",
+           "gpe_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(INCLUDE),
          "--expt-relaxed-constexpr"]

@@ -25,6 +25,14 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+}  // namespace
+
+namespace gpe {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace gpe
+
+namespace {
+
 #define CU(call)                                                                            \
   do {                                                                                      \
     cudaError_t e_ = (call);                                                                \

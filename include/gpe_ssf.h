@@ -163,6 +163,18 @@ int  gpe_profile_read(gpe_plan* plan, double* ms, long long* count);
 /* device status word: bit 0 non-finite norm, bit 1 timeout; read and clear (synchronises) */
 int  gpe_status(gpe_plan* plan, int* flags, void* stream);
 
+/* Renormalise psi in place (psi /= sqrt(N), N = dx^3 sum |psi|^2) without allocating
+ * any device memory and without a plan.  No counterpart in the reference: it is for
+ * callers that cannot call cudaMalloc -- host frameworks whose memory pool already
+ * owns the free HBM, plugin hosts that forbid allocation inside their step callbacks.
+ * The reduction scratch is a fixed 16 KiB file-scope device array per GPU (held
+ * until the process exits).  Limit: n <= 1024 (2^30 points); larger grids are
+ * rejected with GPE_ERR_UNSUPPORTED.  All calls on a device share that array, so
+ * calls that overlap on the GPU race; the first call on each device looks up the
+ * array's address and should come before any stream capture.  norm (nullable, host)
+ * receives N and then the call synchronises `stream`. */
+int  gpe_normalise_noalloc(void* psi, int n, int dtype, double dx, double* norm, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
