@@ -63,6 +63,12 @@ SIGNATURES = {
     "gpe_launch_count": [_vp, _llp],
     "gpe_profile": [_vp, ctypes.c_int],
     "gpe_profile_read": [_vp, _dp, _llp],
+    "gpe_batch_create": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(_vp)],
+    "gpe_batch_destroy": [_vp],
+    "gpe_batch_bind": [_vp, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int), _vp],
+    "gpe_batch_step": [_vp, ctypes.c_int, _vp],
+    "gpe_batch_diagnostics": [_vp, _dp, _vp],
+    "gpe_batch_launch_count": [_vp, _llp],
     "gpe_normalise_noalloc": [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _vp],
 }
 

@@ -1,0 +1,178 @@
+"""Batched imaginary-time ground-state solves of mixed grid sizes.
+
+Many independent solves (sweeps over g, trap aspect ratios and grid sizes)
+advance together: ``gpe_batch_*`` groups the instances by grid size, launches
+every sweep once per group over (tiles x instances), and replays one step of
+all groups from a CUDA graph with a parallel branch per group.  Each instance
+runs exactly the arithmetic of its own single-plan step, so a solve gives the
+same bits alone and in the batch.
+
+:func:`solve` runs every instance until ``|E_k - E_{k-K}| / (K |E_k|) < tol``
+(energy change per step, checked every ``K`` steps) or ``max_steps``, retiring
+converged instances from the batch as it goes.
+"""
+
+import ctypes
+from dataclasses import dataclass, field
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .expressions import split_static
+from .plan import _DTYPES, _dptr, _stream
+
+
+@dataclass
+class Instance:
+    """One solve, in reference units (kinetic factor ``exp(-i c k^2 dt)``)."""
+    n: int
+    simulation_range: float
+    beta: float
+    dt: float
+    static_expr: str = "0"
+    kinetic_coeff: float = 1.0
+    x: np.ndarray = field(init=False, repr=False)
+    k: np.ndarray = field(init=False, repr=False)
+
+    def __post_init__(self):
+        L = self.simulation_range
+        self.x = np.linspace(-L / 2, L / 2, self.n, endpoint=False)
+        self.k = 2 * np.pi * np.fft.fftfreq(self.n, L / self.n)
+
+
+class Batch:
+    def __init__(self, instances, dtype=torch.complex64):
+        if not torch.cuda.is_available():
+            raise RuntimeError("gpe_simulator_b200 needs a CUDA device (sm_100a)")
+        self.lib = _lib.load()
+        self.instances = list(instances)
+        self.dtype = dtype
+        count = len(self.instances)
+        descs = (_lib.Desc * count)()
+        self._keep = []
+        for d, inst in zip(descs, self.instances):
+            d.n, d.dtype, d.kind = inst.n, _DTYPES[dtype], _lib.IMAGINARY
+            d.beta, d.dt, d.kinetic_coeff = float(inst.beta), float(inst.dt), float(inst.kinetic_coeff)
+            a, d.x_array = _dptr(inst.x)
+            self._keep.append(a)
+            a, d.k_array = _dptr(inst.k)
+            self._keep.append(a)
+            for name, prog in zip(("static_x", "static_y", "static_z", "static_g"),
+                                  split_static(inst.static_expr)):
+                if prog:
+                    a, ptr = _dptr(prog)
+                    self._keep.append(a)
+                    setattr(d, name, ptr)
+                    setattr(d, name + "_len", len(prog))
+        handle = ctypes.c_void_p()
+        _lib.check(self.lib.gpe_batch_create(ctypes.cast(descs, ctypes.c_void_p), count, ctypes.byref(handle)))
+        self._h = handle
+        self.psis = [None] * count
+        self.active = np.ones(count, np.int32)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            torch.cuda.synchronize()
+            self.lib.gpe_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bind(self, psis, active=None):
+        """Device states of every instance (C-contiguous cubes) and the active mask."""
+        for i, (p, inst) in enumerate(zip(psis, self.instances)):
+            if p is not None:
+                if (not isinstance(p, torch.Tensor) or not p.is_cuda or p.dtype != self.dtype
+                        or tuple(p.shape) != (inst.n,) * 3 or not p.is_contiguous()):
+                    raise AssertionError(f"psi {i} must be a contiguous {self.dtype} CUDA cube of side {inst.n}")
+        self.psis = list(psis)
+        if active is not None:
+            self.active = np.asarray(active, np.int32).copy()
+        ptrs = (ctypes.c_void_p * len(psis))(*[p.data_ptr() if p is not None else None for p in psis])
+        act = self.active.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        _lib.check(self.lib.gpe_batch_bind(self._h, ptrs, act, _stream()))
+
+    def step(self, nsteps):
+        _lib.check(self.lib.gpe_batch_step(self._h, int(nsteps), _stream()))
+
+    def diagnostics(self):
+        """``(count, 6)`` array of N, E_kin, E_pot, E_int, E, mu (NaN for unbound instances)."""
+        out = np.full((len(self.instances), 6), np.nan)
+        _lib.check(self.lib.gpe_batch_diagnostics(
+            self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream()))
+        return out
+
+    def launch_count(self):
+        out = ctypes.c_longlong()
+        _lib.check(self.lib.gpe_batch_launch_count(self._h, ctypes.byref(out)))
+        return out.value
+
+    def solve(self, psis, tol=1e-9, max_steps=5000, check_every=10):
+        """Run every instance to ``|dE|/E < tol`` per step or ``max_steps``.
+
+        Returns ``(steps, energies)``: steps taken and final diagnostics per instance.
+        """
+        count = len(self.instances)
+        self.bind(psis, np.ones(count, np.int32))
+        steps = np.zeros(count, np.int64)
+        last = self.diagnostics()[:, 4]
+        done = np.zeros(count, bool)
+        final = np.full((count, 6), np.nan)
+        while not done.all():
+            chunk = int(min(check_every, max_steps - steps[~done].max()))
+            if chunk <= 0:
+                break
+            self.step(chunk)
+            steps[~done] += chunk
+            diag = self.diagnostics()
+            e = diag[:, 4]
+            with np.errstate(invalid="ignore", divide="ignore"):
+                rate = np.abs(e - last) / (chunk * np.abs(e))
+            newly = (~done) & ((rate < tol) | (steps >= max_steps))
+            final[newly] = diag[newly]
+            last = np.where(done, last, e)
+            if newly.any():
+                done |= newly
+                if not done.all():
+                    self.bind(self.psis, (~done).astype(np.int32))
+        return steps, final
+
+
+def sweep_instances(count=64, seed=1, dt=1e-3):
+    """The batched parameter sweep, in reference units.
+
+    Grid side drawn from {48, 64, 96, 128, 160} with box [-L, L) for L in
+    {6, 8, 10, 12, 14}; g log-uniform in [100, 5000]; lambda_y, lambda_z uniform
+    in [0.5, 2]; V = (x^2 + lambda_y^2 y^2 + lambda_z^2 z^2)/2 and oscillator time
+    step ``dt``.  Mapped exactly onto the reference convention: V x2, g x2, dt/2.
+    """
+    rng = np.random.default_rng(seed)
+    sizes = [(48, 6.0), (64, 8.0), (96, 10.0), (128, 12.0), (160, 14.0)]
+    out = []
+    for _ in range(count):
+        n, L = sizes[rng.integers(len(sizes))]
+        g = float(math.exp(rng.uniform(math.log(100.0), math.log(5000.0))))
+        ly, lz = rng.uniform(0.5, 2.0, 2)
+        expr = f"x**2+{float(ly * ly)!r}*y**2+{float(lz * lz)!r}*z**2"
+        out.append(Instance(n=n, simulation_range=2 * L, beta=2 * g, dt=dt / 2, static_expr=expr))
+    return out
+
+
+def initial_states(instances, dtype=torch.complex64, seed0=100, device="cuda"):
+    """Seeded normalised Gaussian x (1 + 0.01 complex noise) for every instance."""
+    out = []
+    for i, inst in enumerate(instances):
+        n, x = inst.n, inst.x
+        rng = np.random.default_rng(seed0 + i)
+        g = np.exp(-x ** 2 / 2)
+        psi = g[:, None, None] * g[None, :, None] * g[None, None, :]
+        psi = psi * (1 + 0.01 * (rng.standard_normal((n, n, n)) + 1j * rng.standard_normal((n, n, n))) / np.sqrt(2))
+        psi /= np.sqrt(np.sum(np.abs(psi) ** 2) * (x[1] - x[0]) ** 3)
+        out.append(torch.from_numpy(psi.astype(np.complex128)).to(device).to(dtype).contiguous())
+    return out

@@ -492,7 +492,7 @@ __device__ __forceinline__ void fast_store(const typename Cx<R>::T (&v)[EPT], co
 //   FM_Z21    inverse, 1/M, half(t1), half(t2), forward             last z of a step + first z of the next
 //   FM_XKIN   forward, kinetic, inverse                             x sweep
 template <int N, int AX, typename R, int MODE>
-__global__ void __launch_bounds__(FastCfg<N, R>::T) k_fast(Phys ph, Sweep sw, FastOps op) {
+__device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const FastOps& op) {
   using C = typename Cx<R>::T;
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
@@ -568,6 +568,25 @@ __global__ void __launch_bounds__(FastCfg<N, R>::T) k_fast(Phys ph, Sweep sw, Fa
     block_merge<1>(a, red);
     norm_finish(ph, sw, a[0], red);
   }
+}
+
+template <int N, int AX, typename R, int MODE>
+__global__ void __launch_bounds__(FastCfg<N, R>::T) k_fast(Phys ph, Sweep sw, FastOps op) {
+  fast_body<N, AX, R, MODE>(ph, sw, op);
+}
+
+// Batched launch: blockIdx.y selects the instance (structs staged in shared memory).
+template <int N, int AX, typename R, int MODE>
+__global__ void __launch_bounds__(FastCfg<N, R>::T) k_fast_batch(const Phys* __restrict__ phs,
+                                                                const Sweep* __restrict__ sws, FastOps op) {
+  __shared__ Phys ph;
+  __shared__ Sweep sw;
+  if (threadIdx.x == 0) {
+    ph = phs[blockIdx.y];
+    sw = sws[blockIdx.y];
+  }
+  __syncthreads();
+  fast_body<N, AX, R, MODE>(ph, sw, op);
 }
 
 }  // namespace gpe

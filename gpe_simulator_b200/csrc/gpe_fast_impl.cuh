@@ -38,6 +38,52 @@ static cudaError_t launch_fast_n(int ax, const Phys& ph, const Sweep& sw, const 
   return launch_fast_one<N, FX, R, FM_PLAIN>(ph, sw, op, st);
 }
 
+template <int N, int AX, typename R, int MODE>
+static cudaError_t launch_fastb_one(const Phys* phs, const Sweep* sws, int count, const FastOps& op,
+                                    cudaStream_t st) {
+  constexpr int L = FastCfg<N, R>::L;
+  constexpr int T = FastCfg<N, R>::T;
+  const int tiles = AX == FZ ? N * N / L : N * (N / L);
+  constexpr size_t smem = fast_smem_bytes<N, R>();
+  static int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaError_t e = cudaFuncSetAttribute(k_fast_batch<N, AX, R, MODE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_dev = dev;
+  }
+  k_fast_batch<N, AX, R, MODE><<<dim3(tiles, count), T, smem, st>>>(phs, sws, op);
+  return cudaGetLastError();
+}
+
+template <int N, typename R>
+static cudaError_t launch_fastb_n(int ax, const Phys* phs, const Sweep* sws, int count, const FastOps& op,
+                                  cudaStream_t st) {
+  switch (op.mode) {
+    case FM_Z1: return launch_fastb_one<N, FZ, R, FM_Z1>(phs, sws, count, op, st);
+    case FM_Z2: return launch_fastb_one<N, FZ, R, FM_Z2>(phs, sws, count, op, st);
+    case FM_Z21: return launch_fastb_one<N, FZ, R, FM_Z21>(phs, sws, count, op, st);
+    case FM_XKIN: return launch_fastb_one<N, FX, R, FM_XKIN>(phs, sws, count, op, st);
+    default: break;
+  }
+  if (ax == FZ) return launch_fastb_one<N, FZ, R, FM_PLAIN>(phs, sws, count, op, st);
+  if (ax == FY) return launch_fastb_one<N, FY, R, FM_PLAIN>(phs, sws, count, op, st);
+  return launch_fastb_one<N, FX, R, FM_PLAIN>(phs, sws, count, op, st);
+}
+
+template <typename R>
+cudaError_t launch_fast_batch(int n, int ax, const Phys* phs, const Sweep* sws, int count, const FastOps& op,
+                              cudaStream_t st) {
+  switch (n) {
+    case 64: return launch_fastb_n<64, R>(ax, phs, sws, count, op, st);
+    case 128: return launch_fastb_n<128, R>(ax, phs, sws, count, op, st);
+    case 256: return launch_fastb_n<256, R>(ax, phs, sws, count, op, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 template <typename R>
 cudaError_t launch_fast(int n, int ax, const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st) {
   switch (n) {

@@ -408,7 +408,7 @@ static __device__ void norm_finish(const Phys& ph, const Sweep& sw, Acc total, A
 
 // ---------------------------------------------------------------- the sweep kernel
 template <typename R, int AX, int EPT, bool GEN>
-__global__ void __launch_bounds__(512, 1) k_sweep(Phys ph, Sweep sw) {
+__device__ __forceinline__ void sweep_body(const Phys& ph, const Sweep& sw) {
   using C = typename Cx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = sw.pp.n;
@@ -494,6 +494,26 @@ __global__ void __launch_bounds__(512, 1) k_sweep(Phys ph, Sweep sw) {
         sw.hist[(long long)blockIdx.x * sw.nbins + b] = cx.hist[b];
     }
   }
+}
+
+// Single-plan launch (structs by value) and batched launch: blockIdx.y selects the
+// instance whose structs are staged once into shared memory.
+template <typename R, int AX, int EPT, bool GEN>
+__global__ void __launch_bounds__(512, 1) k_sweep(Phys ph, Sweep sw) {
+  sweep_body<R, AX, EPT, GEN>(ph, sw);
+}
+
+template <typename R, int AX, int EPT, bool GEN>
+__global__ void __launch_bounds__(512, 1) k_sweep_batch(const Phys* __restrict__ phs,
+                                                         const Sweep* __restrict__ sws) {
+  __shared__ Phys ph;
+  __shared__ Sweep sw;
+  if (threadIdx.x == 0) {
+    ph = phs[blockIdx.y];
+    sw = sws[blockIdx.y];
+  }
+  __syncthreads();
+  sweep_body<R, AX, EPT, GEN>(ph, sw);
 }
 
 }  // namespace gpe

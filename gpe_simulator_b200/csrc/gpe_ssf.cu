@@ -6,6 +6,9 @@
 namespace gpe {
 template <typename R>
 cudaError_t launch_fast(int n, int ax, const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st);
+template <typename R>
+cudaError_t launch_fast_batch(int n, int ax, const Phys* phs, const Sweep* sws, int count, const FastOps& op,
+                              cudaStream_t st);
 }
 
 #include <cmath>
@@ -41,6 +44,8 @@ namespace {
       return fail(GPE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
     }                                                                                       \
   } while (0)
+
+#define TRY(x) do { int r_ = (x); if (r_ != GPE_OK) return r_; } while (0)
 
 // Host evaluation of a potential program (same semantics as eval_program).
 double host_eval(const std::vector<double>& prog, double x, double y, double z, double t) {
@@ -229,8 +234,9 @@ int tiles_of(const gpe_plan* p, int ax) {
   return n * ((n + p->lt_yx - 1) / p->lt_yx);
 }
 
+// Plan-owned pointers of a generic sweep and its launch geometry.
 template <typename R>
-int launch(gpe_plan* p, int ax, Sweep sw, cudaStream_t st) {
+int sweep_geometry(const gpe_plan* p, int ax, Sweep& sw, int& tiles, int& threads, size_t& smem) {
   using C = typename Cx<R>::T;
   const int n = p->n;
   sw.pp = p->pp;
@@ -244,18 +250,25 @@ int launch(gpe_plan* p, int ax, Sweep sw, cudaStream_t st) {
   int lt = ax == AX_Z ? p->lt_z : p->lt_yx;
   sw.lt = lt;
   sw.tiles_per_row = (n + p->lt_yx - 1) / p->lt_yx;
-  const int tiles = tiles_of(p, ax);
+  tiles = tiles_of(p, ax);
   const int pitch = ax == AX_Z ? ((n & 1) ? n : n + 1) : lt;
   const int tile_elems = ax == AX_Z ? lt * pitch : n * lt;
   const int E = n * lt;
-  int threads = (E + p->ept - 1) / p->ept;
+  threads = (E + p->ept - 1) / p->ept;
   threads = ((threads + 31) / 32) * 32;
   if (threads < 32) threads = 32;
   if (threads > 512) return fail(GPE_ERR_UNSUPPORTED, "tile too large");
-  size_t smem = (size_t)(2 * n + tile_elems) * sizeof(C) + 32 * 4 * sizeof(Acc) + (size_t)p->nbins * sizeof(double);
+  smem = (size_t)(2 * n + tile_elems) * sizeof(C) + 32 * 4 * sizeof(Acc) + (size_t)p->nbins * sizeof(double);
   if (smem > 200 * 1024) return fail(GPE_ERR_UNSUPPORTED, "tile does not fit in shared memory");
+  return GPE_OK;
+}
+
+template <typename R>
+int launch(gpe_plan* p, int ax, Sweep sw, cudaStream_t st) {
+  int tiles = 0, threads = 0;
+  size_t smem = 0;
+  TRY(sweep_geometry<R>(p, ax, sw, tiles, threads, smem));
   CU(launch_sweep<R>(ax, p->gen, p->ph, sw, tiles, threads, smem, st));
-  CU(cudaGetLastError());
   return GPE_OK;
 }
 
@@ -329,7 +342,6 @@ Sweep mk_sweep(const void* src, void* dst) {
 // reference: t = i*dt (gpe/launch.py:10), t_mid = t + dt/2 (gpe/make_propagator.py:94)
 double t_mid_host(const gpe_plan* p, long long step) { return (double)step * p->dt + p->dt / 2; }
 
-#define TRY(x) do { int r_ = (x); if (r_ != GPE_OK) return r_; } while (0)
 
 // Norm of psi into d_scale (sqrtN, 1/sqrtN, N) via a no-store sweep.
 int norm_sweep(gpe_plan* p, const void* psi, cudaStream_t st) {
@@ -674,6 +686,42 @@ int finish_diag(gpe_plan* p, int na, bool hist, std::vector<double>& host, cudaS
   return GPE_OK;
 }
 
+// The three diagnostic sweeps of psi at time t (real-space sums in the z sweep
+// writing the partial transform to the plan's work buffer, k-space sums and
+// shells in the x sweep); results stay on the device until finish_diag.
+int diag_launch(gpe_plan* p, const void* psi, double t, cudaStream_t st) {
+  Sweep s = mk_sweep(psi, p->d_work);
+  s.pre = PW_DIAG_R;
+  s.t1 = t;
+  s.fft1 = 1;
+  s.partial = p->d_partial;
+  TRY(sweep(p, AX_Z, s, st));
+  s = mk_sweep(p->d_work, p->d_work);
+  s.fft1 = 1;
+  TRY(sweep(p, AX_Y, s, st));
+  s = mk_sweep(p->d_work, nullptr);
+  s.fft1 = 1;
+  s.post = PW_DIAG_K;
+  s.partial = p->d_partial + 4 * (size_t)p->max_tiles;
+  s.hist = p->d_hist;
+  return sweep(p, AX_X, s, st);
+}
+
+// {N, E_kin, E_pot, E_int, E, mu} from the finished sums h[0..3].
+void diag_scalars(const gpe_plan* p, const double* h, double* scalars) {
+  const double dx3 = p->ph.dx3;
+  const double N = h[0] * dx3;
+  const double e_kin = p->ckin * h[3] * dx3 * p->ph.inv_m;
+  const double e_pot = h[1] * dx3;
+  const double e_int = 0.5 * p->beta * h[2] * dx3;
+  scalars[0] = N;
+  scalars[1] = e_kin;
+  scalars[2] = e_pot;
+  scalars[3] = e_int;
+  scalars[4] = e_kin + e_pot + e_int;
+  scalars[5] = (e_kin + e_pot + 2.0 * e_int) / N;
+}
+
 }  // namespace
 
 // ================================================================ C ABI
@@ -816,37 +864,13 @@ int gpe_diagnostics(gpe_plan* p, const void* psi, double t, double* scalars, dou
   cudaStream_t st = (cudaStream_t)stream;
   TRY(ensure_work(p));
   TRY(ensure_hist(p));
-  Sweep s = mk_sweep(psi, p->d_work);
-  s.pre = PW_DIAG_R;
-  s.t1 = t;
-  s.fft1 = 1;
-  s.partial = p->d_partial;
-  TRY(sweep(p, AX_Z, s, st));
+  TRY(diag_launch(p, psi, t, st));
   const int na = tiles_of(p, AX_Z);
-  s = mk_sweep(p->d_work, p->d_work);
-  s.fft1 = 1;
-  TRY(sweep(p, AX_Y, s, st));
-  s = mk_sweep(p->d_work, nullptr);
-  s.fft1 = 1;
-  s.post = PW_DIAG_K;
-  s.partial = p->d_partial + 4 * (size_t)p->max_tiles;
-  s.hist = p->d_hist;
-  TRY(sweep(p, AX_X, s, st));
   std::vector<double> h;
   TRY(finish_diag(p, na, nk != nullptr, h, st));
-  const double dx3 = p->ph.dx3;
-  const double N = h[0] * dx3;
-  const double e_kin = p->ckin * h[3] * dx3 * p->ph.inv_m;
-  const double e_pot = h[1] * dx3;
-  const double e_int = 0.5 * p->beta * h[2] * dx3;
-  scalars[0] = N;
-  scalars[1] = e_kin;
-  scalars[2] = e_pot;
-  scalars[3] = e_int;
-  scalars[4] = e_kin + e_pot + e_int;
-  scalars[5] = (e_kin + e_pot + 2.0 * e_int) / N;
+  diag_scalars(p, h.data(), scalars);
   if (nk)
-    for (int b = 0; b < p->nbins; ++b) nk[b] = h[4 + b] * dx3 * p->ph.inv_m;
+    for (int b = 0; b < p->nbins; ++b) nk[b] = h[4 + b] * p->ph.dx3 * p->ph.inv_m;
   if (counts)
     for (int b = 0; b < p->nbins; ++b) counts[b] = p->counts[b];
   return GPE_OK;
@@ -886,6 +910,303 @@ int gpe_status(gpe_plan* p, int* flags, void* stream) {
   CU(cudaMemcpyAsync(flags, p->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
   CU(cudaMemsetAsync(p->d_status, 0, sizeof(int), st));
   CU(cudaStreamSynchronize(st));
+  return GPE_OK;
+}
+
+}  // extern "C"
+
+// ================================================================ batches
+// Many independent imaginary-time solves of mixed grid sizes advanced together.
+// Instances are grouped by grid size; every sweep of a step is one launch per
+// group whose grid is (tiles, instances): blockIdx.y picks the instance, whose
+// physics and pointers come from device arrays.  One Strang step of all groups
+// is captured once as a CUDA graph with one parallel branch per group and
+// replayed for every further step.
+struct gpe_batch {
+  int dtype = 0;
+  std::vector<gpe_plan*> plans;
+  struct Group {
+    int n = 0;
+    bool fast = false;
+    std::vector<int> all;       // every instance of this size
+    std::vector<int> members;   // the bound (active) ones
+    Phys* d_ph = nullptr;
+    Sweep* d_sw = nullptr;      // [roles][members]
+    int cap = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+  };
+  std::vector<Group> groups;
+  std::vector<void*> psis;
+  cudaGraphExec_t graph = nullptr;
+  cudaGraph_t graph_def = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaStream_t cap = nullptr;   // private stream the step graph is captured on
+  cudaEvent_t ready = nullptr;
+  double* h_sums = nullptr;     // pinned, 4 doubles per instance
+  long long launches = 0;
+};
+
+namespace {
+
+enum { ROLE_Z1N = 0, ROLE_Z1, ROLE_Y1, ROLE_X, ROLE_Y2, ROLE_Z2, ROLE_SC, ROLE_COUNT };
+
+void batch_free_graph(gpe_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->graph_def) cudaGraphDestroy(b->graph_def);
+  b->graph = nullptr;
+  b->graph_def = nullptr;
+}
+
+void batch_free(gpe_batch* b) {
+  batch_free_graph(b);
+  for (auto& g : b->groups) {
+    if (g.d_ph) cudaFree(g.d_ph);
+    if (g.d_sw) cudaFree(g.d_sw);
+    if (g.stream) cudaStreamDestroy(g.stream);
+    if (g.ev) cudaEventDestroy(g.ev);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->ready) cudaEventDestroy(b->ready);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  if (b->h_sums) cudaFreeHost(b->h_sums);
+  for (auto* p : b->plans) free_plan(p);
+  delete b;
+}
+
+Sweep role_sweep(int role, void* psi, gpe_plan* p) {
+  Sweep s = mk_sweep(psi, psi);
+  s.partial = p->d_partial;
+  s.t1 = s.t2 = p->dt / 2;
+  switch (role) {
+    case ROLE_Z1N: s.pre = PW_HALF1; s.fft1 = 1; break;
+    case ROLE_Z1: s.pre = PW_HALF1 | PW_SCALE; s.fft1 = 1; break;
+    case ROLE_Y1: s.fft1 = 1; break;
+    case ROLE_X: s.fft1 = 1; s.mid = PW_KIN | PW_CONJ_LAST; s.fft2 = 1; s.post = PW_CONJ_FIRST; break;
+    case ROLE_Y2: s.pre = PW_CONJ_LAST; s.fft1 = 1; s.post = PW_CONJ_FIRST; break;
+    case ROLE_Z2: s.pre = PW_CONJ_LAST; s.fft1 = 1; s.post = PW_CONJ_FIRST | PW_INVM | PW_HALF1 | PW_NORM; break;
+    default: s.pre = PW_SCALE; break;
+  }
+  return s;
+}
+
+int role_axis(int role) {
+  if (role == ROLE_Y1 || role == ROLE_Y2) return AX_Y;
+  if (role == ROLE_X) return AX_X;
+  return AX_Z;
+}
+
+template <typename R>
+int group_launch(gpe_batch* b, gpe_batch::Group& g, int role, cudaStream_t st) {
+  const int count = (int)g.members.size();
+  if (!count) return GPE_OK;
+  const Sweep* sws = g.d_sw + (size_t)role * count;
+  const int ax = role_axis(role);
+  if (g.fast && role != ROLE_SC) {
+    FastOps op = mk_ops(FM_PLAIN);
+    const int fax = ax == AX_Z ? FZ : ax == AX_Y ? FY : FX;
+    switch (role) {
+      case ROLE_Z1N: op = mk_ops(FM_Z1, 0, 0, 0); break;
+      case ROLE_Z1: op = mk_ops(FM_Z1, 0, 0, 1); break;
+      case ROLE_Y1: op = mk_ops(FM_PLAIN); break;
+      case ROLE_X: op = mk_ops(FM_XKIN); break;
+      case ROLE_Y2: op = mk_ops(FM_PLAIN, 1); break;
+      default: op = mk_ops(FM_Z2, 0, 0, 0, 1); break;
+    }
+    CU(launch_fast_batch<R>(g.n, fax, g.d_ph, sws, count, op, st));
+  } else {
+    gpe_plan* p = b->plans[g.members[0]];
+    Sweep geo = mk_sweep(nullptr, nullptr);
+    int tiles = 0, threads = 0;
+    size_t smem = 0;
+    TRY(sweep_geometry<R>(p, ax, geo, tiles, threads, smem));
+    CU(launch_sweep_batch<R>(ax, p->gen, g.d_ph, sws, count, tiles, threads, smem, st));
+  }
+  ++b->launches;
+  return GPE_OK;
+}
+
+int group_role(gpe_batch* b, gpe_batch::Group& g, int role, cudaStream_t st) {
+  return b->dtype == GPE_C64 ? group_launch<float>(b, g, role, st) : group_launch<double>(b, g, role, st);
+}
+
+int group_step(gpe_batch* b, gpe_batch::Group& g, bool scaled, cudaStream_t st) {
+  TRY(group_role(b, g, scaled ? ROLE_Z1 : ROLE_Z1N, st));
+  TRY(group_role(b, g, ROLE_Y1, st));
+  TRY(group_role(b, g, ROLE_X, st));
+  TRY(group_role(b, g, ROLE_Y2, st));
+  return group_role(b, g, ROLE_Z2, st);
+}
+
+// Every group's step on its own stream, forked from and joined back into `st`.
+int batch_step_all(gpe_batch* b, bool scaled, cudaStream_t st) {
+  CU(cudaEventRecord(b->fork, st));
+  for (auto& g : b->groups) {
+    if (g.members.empty()) continue;
+    CU(cudaStreamWaitEvent(g.stream, b->fork, 0));
+    TRY(group_step(b, g, scaled, g.stream));
+    CU(cudaEventRecord(g.ev, g.stream));
+    CU(cudaStreamWaitEvent(st, g.ev, 0));
+  }
+  return GPE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpe_batch_create(const gpe_desc* descs, int count, gpe_batch** out) {
+  if (!descs || !out || count <= 0) return fail(GPE_ERR_ARG, "descs, count > 0 and out are required");
+  *out = nullptr;
+  gpe_batch* b = new gpe_batch();
+  b->dtype = descs[0].dtype;
+  for (int i = 0; i < count; ++i) {
+    if (descs[i].kind != GPE_IMAGINARY) { batch_free(b); return fail(GPE_ERR_ARG, "batches hold imaginary-time solves"); }
+    if (descs[i].dtype != b->dtype) { batch_free(b); return fail(GPE_ERR_ARG, "all instances of a batch share one dtype"); }
+    gpe_plan* p = nullptr;
+    const int rc = create(&descs[i], &p);
+    if (rc != GPE_OK) { batch_free(b); return rc; }
+    b->plans.push_back(p);
+    int gi = -1;
+    for (size_t q = 0; q < b->groups.size(); ++q)
+      if (b->groups[q].n == p->n) gi = (int)q;
+    if (gi < 0) {
+      gpe_batch::Group g;
+      g.n = p->n;
+      g.fast = p->fast;
+      b->groups.push_back(g);
+      gi = (int)b->groups.size() - 1;
+    }
+    b->groups[gi].all.push_back(i);
+  }
+  for (auto& g : b->groups) {
+    CU(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+    CU(cudaEventCreateWithFlags(&g.ev, cudaEventDisableTiming));
+  }
+  CU(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&b->ready, cudaEventDisableTiming));
+  CU(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+  CU(cudaMallocHost(&b->h_sums, sizeof(double) * 4 * count));
+  b->psis.assign(count, nullptr);
+  *out = b;
+  return GPE_OK;
+}
+
+int gpe_batch_destroy(gpe_batch* b) {
+  if (!b) return GPE_OK;
+  cudaDeviceSynchronize();
+  batch_free(b);
+  return GPE_OK;
+}
+
+int gpe_batch_bind(gpe_batch* b, void* const* psis, const int* active, void* stream) {
+  if (!b || !psis) return fail(GPE_ERR_ARG, "null argument");
+  const int count = (int)b->plans.size();
+  CU(cudaStreamSynchronize((cudaStream_t)stream));
+  for (auto& g : b->groups) CU(cudaStreamSynchronize(g.stream));
+  batch_free_graph(b);
+  for (int i = 0; i < count; ++i) b->psis[i] = psis[i];
+  for (auto& g : b->groups) {
+    g.members.clear();
+    for (int i : g.all)
+      if ((!active || active[i]) && psis[i]) g.members.push_back(i);
+    const int m = (int)g.members.size();
+    if (!m) continue;
+    if (m > g.cap) {
+      if (g.d_ph) cudaFree(g.d_ph);
+      if (g.d_sw) cudaFree(g.d_sw);
+      g.d_ph = nullptr;
+      g.d_sw = nullptr;
+      CU(cudaMalloc(&g.d_ph, sizeof(Phys) * m));
+      CU(cudaMalloc(&g.d_sw, sizeof(Sweep) * m * ROLE_COUNT));
+      g.cap = m;
+    }
+    std::vector<Phys> hph(m);
+    std::vector<Sweep> hsw((size_t)m * ROLE_COUNT);
+    for (int q = 0; q < m; ++q) {
+      gpe_plan* p = b->plans[g.members[q]];
+      TRY(ensure_work(p));
+      TRY(ensure_hist(p));
+      hph[q] = p->ph;
+      for (int role = 0; role < ROLE_COUNT; ++role) {
+        Sweep s = role_sweep(role, psis[g.members[q]], p);
+        int tiles = 0, threads = 0;
+        size_t smem = 0;
+        const int rc = b->dtype == GPE_C64 ? sweep_geometry<float>(p, role_axis(role), s, tiles, threads, smem)
+                                           : sweep_geometry<double>(p, role_axis(role), s, tiles, threads, smem);
+        if (rc != GPE_OK) return rc;
+        hsw[(size_t)role * m + q] = s;
+      }
+    }
+    CU(cudaMemcpy(g.d_ph, hph.data(), sizeof(Phys) * m, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(g.d_sw, hsw.data(), sizeof(Sweep) * m * ROLE_COUNT, cudaMemcpyHostToDevice));
+  }
+  return GPE_OK;
+}
+
+int gpe_batch_step(gpe_batch* b, int nsteps, void* stream) {
+  if (!b) return fail(GPE_ERR_ARG, "null batch");
+  if (nsteps <= 0) return GPE_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  bool any = false;
+  for (auto& g : b->groups) any = any || !g.members.empty();
+  if (!any) return GPE_OK;
+  TRY(batch_step_all(b, false, st));  // first step: psi is normalised, no pending scale
+  if (nsteps > 1) {
+    if (!b->graph) {
+      // capture on the batch's own stream (the caller's may be the legacy default stream)
+      CU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+      const int rc = batch_step_all(b, true, b->cap);
+      cudaGraph_t gdef = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(b->cap, &gdef);
+      if (rc != GPE_OK) { if (gdef) cudaGraphDestroy(gdef); return rc; }
+      CU(e);
+      b->graph_def = gdef;
+      CU(cudaGraphInstantiate(&b->graph, gdef, 0));
+    }
+    for (int s = 1; s < nsteps; ++s) CU(cudaGraphLaunch(b->graph, st));
+  }
+  // apply the last renormalisation
+  CU(cudaEventRecord(b->fork, st));
+  for (auto& g : b->groups) {
+    if (g.members.empty()) continue;
+    CU(cudaStreamWaitEvent(g.stream, b->fork, 0));
+    TRY(group_role(b, g, ROLE_SC, g.stream));
+    CU(cudaEventRecord(g.ev, g.stream));
+    CU(cudaStreamWaitEvent(st, g.ev, 0));
+  }
+  return GPE_OK;
+}
+
+int gpe_batch_diagnostics(gpe_batch* b, double* scalars, void* stream) {
+  if (!b || !scalars) return fail(GPE_ERR_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int count = (int)b->plans.size();
+  for (int i = 0; i < count; ++i) {
+    bool bound = false;
+    for (auto& g : b->groups)
+      for (int m : g.members) bound = bound || m == i;
+    if (!bound) continue;
+    gpe_plan* p = b->plans[i];
+    TRY(diag_launch(p, b->psis[i], 0.0, st));
+    k_finish_diag<<<1, 256, 0, st>>>(p->d_partial, tiles_of(p, AX_Z), p->d_partial + 4 * (size_t)p->max_tiles,
+                                     tiles_of(p, AX_X), nullptr, p->nbins, p->d_out);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(b->h_sums + 4 * i, p->d_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CU(cudaStreamSynchronize(st));
+  for (int i = 0; i < count; ++i) {
+    bool bound = false;
+    for (auto& g : b->groups)
+      for (int m : g.members) bound = bound || m == i;
+    if (bound) diag_scalars(b->plans[i], b->h_sums + 4 * i, scalars + 6 * i);
+  }
+  return GPE_OK;
+}
+
+int gpe_batch_launch_count(const gpe_batch* b, long long* count) {
+  if (!b || !count) return fail(GPE_ERR_ARG, "null argument");
+  *count = b->launches;
   return GPE_OK;
 }
 

@@ -11,4 +11,9 @@ template <typename R>
 cudaError_t launch_sweep(int ax, bool gen, const Phys& ph, const Sweep& sw, int tiles, int threads,
                          size_t smem, cudaStream_t st);
 
+// Batched launch: grid (tiles, count), instance i reads phs[i] and sws[i] (device arrays).
+template <typename R>
+cudaError_t launch_sweep_batch(int ax, bool gen, const Phys* phs, const Sweep* sws, int count, int tiles,
+                               int threads, size_t smem, cudaStream_t st);
+
 }  // namespace gpe

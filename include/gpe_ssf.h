@@ -163,6 +163,24 @@ int  gpe_profile_read(gpe_plan* plan, double* ms, long long* count);
 /* device status word: bit 0 non-finite norm, bit 1 timeout; read and clear (synchronises) */
 int  gpe_status(gpe_plan* plan, int* flags, void* stream);
 
+/* Batches: many independent imaginary-time solves (mixed grid sizes, one dtype)
+ * advanced together.  Instances are grouped by grid size; each sweep is one
+ * launch per group over (tiles x instances), and one step of all groups is
+ * replayed from a CUDA graph with a parallel branch per group.  Replaces calling
+ * standard_imaginary_step (gpe/make_propagator.py:109-151) for each solve in turn.
+ *   gpe_batch_bind: psi pointers of every instance (device, C-contiguous) and an
+ *     optional active mask (NULL = all); rebinding discards the captured graph.
+ *   gpe_batch_step: nsteps renormalised steps of every bound instance.
+ *   gpe_batch_diagnostics: scalars[6*i .. 6*i+5] = {N, E_kin, E_pot, E_int, E, mu}
+ *     of every bound instance i (synchronises). */
+typedef struct gpe_batch gpe_batch;
+int  gpe_batch_create(const gpe_desc* descs, int count, gpe_batch** batch);
+int  gpe_batch_destroy(gpe_batch* batch);
+int  gpe_batch_bind(gpe_batch* batch, void* const* psis, const int* active, void* stream);
+int  gpe_batch_step(gpe_batch* batch, int nsteps, void* stream);
+int  gpe_batch_diagnostics(gpe_batch* batch, double* scalars, void* stream);
+int  gpe_batch_launch_count(const gpe_batch* batch, long long* count);
+
 /* Renormalise psi in place (psi /= sqrt(N), N = dx^3 sum |psi|^2) without allocating
  * any device memory and without a plan.  No counterpart in the reference: it is for
  * callers that cannot call cudaMalloc -- host frameworks whose memory pool already

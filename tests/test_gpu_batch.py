@@ -1,0 +1,81 @@
+"""Batched solves: each instance's result is the same alone and in the batch."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ssf
+
+pytestmark = pytest.mark.gpu
+
+
+def small_batch():
+    from gpe_simulator_b200.batch import Instance
+    # mixed sizes: generic (48, 96), register-resident (64, 128) and odd (18)
+    specs = [(48, 12.0, 300.0, "x**2+y**2+z**2"), (64, 12.0, 800.0, "x**2+1.44*y**2+2.25*z**2"),
+             (18, 8.0, 50.0, "x**2+0.5*y**2+2*z**2"), (64, 16.0, 1200.0, "x**2+y**2+4*z**2"),
+             (96, 14.0, 2000.0, "x**2+2*y**2+z**2"), (128, 16.0, 500.0, "x**2+y**2+z**2")]
+    return [Instance(n=n, simulation_range=L, beta=b, dt=5e-4, static_expr=e) for n, L, b, e in specs]
+
+
+@pytest.mark.parametrize("dtype", [torch.complex64, torch.complex128])
+def test_batch_equals_one_at_a_time_bitwise(cuda, dtype):
+    from gpe_simulator_b200 import Plan
+    from gpe_simulator_b200.batch import Batch, initial_states
+    insts = small_batch()
+    states = initial_states(insts, dtype)
+    alone = []
+    for inst, psi in zip(insts, states):
+        p = Plan(inst.n, inst.x, inst.k, dtype=dtype, kind="imaginary", beta=inst.beta, dt=inst.dt,
+                 static_expr=inst.static_expr)
+        a = psi.clone()
+        p.step(a, 25)
+        alone.append(a)
+    b = Batch(insts, dtype)
+    mixed = [s.clone() for s in states]
+    b.bind(mixed)
+    b.step(25)
+    torch.cuda.synchronize()
+    for a, m in zip(alone, mixed):
+        assert torch.equal(a, m)
+    # a subset (active mask) keeps the others untouched and still matches
+    before = [m.clone() for m in mixed]
+    b.bind(mixed, active=[1, 0, 1, 0, 1, 0])
+    b.step(3)
+    torch.cuda.synchronize()
+    for i, (m, s) in enumerate(zip(mixed, before)):
+        assert torch.equal(m, s) == (i % 2 == 1)
+
+
+def test_batch_matches_oracle(cuda):
+    from gpe_simulator_b200.batch import Batch, initial_states
+    insts = small_batch()[:3]
+    states = initial_states(insts, torch.complex128)
+    b = Batch(insts, torch.complex128)
+    work = [s.clone() for s in states]
+    b.bind(work)
+    b.step(30)
+    for inst, s, w in zip(insts, states, work):
+        m = ssf.Model(n=inst.n, simulation_range=inst.simulation_range, kind="imaginary", beta=inst.beta,
+                      dt=inst.dt, static_expr=inst.static_expr)
+        want = ssf.run(s.cpu().numpy(), m, 30)
+        assert ssf.rel_l2(w.cpu().numpy(), want) < 1e-12
+    diag = b.diagnostics()
+    for inst, w, d in zip(insts, work, diag):
+        m = ssf.Model(n=inst.n, simulation_range=inst.simulation_range, kind="imaginary", beta=inst.beta,
+                      dt=inst.dt, static_expr=inst.static_expr)
+        e = ssf.energies(w.cpu().numpy(), m)
+        assert d[0] == pytest.approx(e["N"], rel=1e-12)
+        assert d[4] == pytest.approx(e["E"], rel=1e-10)
+        assert d[5] == pytest.approx(e["mu"], rel=1e-10)
+
+
+def test_solve_converges_and_retires(cuda):
+    from gpe_simulator_b200.batch import Batch, initial_states
+    insts = small_batch()[:4]
+    b = Batch(insts, torch.complex64)
+    states = initial_states(insts, torch.complex64)
+    steps, final = b.solve(states, tol=1e-6, max_steps=3000, check_every=20)
+    assert (steps > 0).all() and (steps <= 3000).all()
+    assert np.isfinite(final).all()
+    np.testing.assert_allclose(final[:, 0], 1.0, atol=1e-5)
