@@ -65,6 +65,8 @@ SIGNATURES = {
     "gpe_profile_read": [_vp, _dp, _llp],
     "gpe_batch_create": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(_vp)],
     "gpe_batch_destroy": [_vp],
+    "gpe_batch_add": [_vp, ctypes.POINTER(Desc), ctypes.POINTER(ctypes.c_int)],
+    "gpe_batch_remove": [_vp, ctypes.c_int],
     "gpe_batch_bind": [_vp, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int), _vp],
     "gpe_batch_step": [_vp, ctypes.c_int, _vp],
     "gpe_batch_diagnostics": [_vp, _dp, _vp],

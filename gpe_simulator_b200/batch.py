@@ -42,6 +42,21 @@ class Instance:
         self.k = 2 * np.pi * np.fft.fftfreq(self.n, L / self.n)
 
 
+def _fill_desc(d, inst, dtype, keep):
+    d.n, d.dtype, d.kind = inst.n, _DTYPES[dtype], _lib.IMAGINARY
+    d.beta, d.dt, d.kinetic_coeff = float(inst.beta), float(inst.dt), float(inst.kinetic_coeff)
+    a, d.x_array = _dptr(inst.x)
+    keep.append(a)
+    a, d.k_array = _dptr(inst.k)
+    keep.append(a)
+    for name, prog in zip(("static_x", "static_y", "static_z", "static_g"), split_static(inst.static_expr)):
+        if prog:
+            a, ptr = _dptr(prog)
+            keep.append(a)
+            setattr(d, name, ptr)
+            setattr(d, name + "_len", len(prog))
+
+
 class Batch:
     def __init__(self, instances, dtype=torch.complex64):
         if not torch.cuda.is_available():
@@ -53,19 +68,7 @@ class Batch:
         descs = (_lib.Desc * count)()
         self._keep = []
         for d, inst in zip(descs, self.instances):
-            d.n, d.dtype, d.kind = inst.n, _DTYPES[dtype], _lib.IMAGINARY
-            d.beta, d.dt, d.kinetic_coeff = float(inst.beta), float(inst.dt), float(inst.kinetic_coeff)
-            a, d.x_array = _dptr(inst.x)
-            self._keep.append(a)
-            a, d.k_array = _dptr(inst.k)
-            self._keep.append(a)
-            for name, prog in zip(("static_x", "static_y", "static_z", "static_g"),
-                                  split_static(inst.static_expr)):
-                if prog:
-                    a, ptr = _dptr(prog)
-                    self._keep.append(a)
-                    setattr(d, name, ptr)
-                    setattr(d, name + "_len", len(prog))
+            _fill_desc(d, inst, dtype, self._keep)
         handle = ctypes.c_void_p()
         _lib.check(self.lib.gpe_batch_create(ctypes.cast(descs, ctypes.c_void_p), count, ctypes.byref(handle)))
         self._h = handle
@@ -84,16 +87,44 @@ class Batch:
         except Exception:
             pass
 
+    def add(self, inst):
+        """Add an instance to the running batch; returns its index (freed indices are reused)."""
+        d = _lib.Desc()
+        keep = []
+        _fill_desc(d, inst, self.dtype, keep)
+        idx = ctypes.c_int()
+        _lib.check(self.lib.gpe_batch_add(self._h, ctypes.byref(d), ctypes.byref(idx)))
+        i = idx.value
+        if i == len(self.instances):
+            self.instances.append(inst)
+            self.psis.append(None)
+            self.active = np.append(self.active, 0).astype(np.int32)
+        else:
+            self.instances[i] = inst
+            self.psis[i] = None
+            self.active[i] = 0
+        return i
+
+    def remove(self, index):
+        """Drop instance ``index`` (its tensors stay with the caller)."""
+        _lib.check(self.lib.gpe_batch_remove(self._h, int(index)))
+        self.instances[index] = None
+        self.psis[index] = None
+        self.active[index] = 0
+
     def bind(self, psis, active=None):
         """Device states of every instance (C-contiguous cubes) and the active mask."""
         for i, (p, inst) in enumerate(zip(psis, self.instances)):
-            if p is not None:
+            if p is not None and inst is not None:
                 if (not isinstance(p, torch.Tensor) or not p.is_cuda or p.dtype != self.dtype
                         or tuple(p.shape) != (inst.n,) * 3 or not p.is_contiguous()):
                     raise AssertionError(f"psi {i} must be a contiguous {self.dtype} CUDA cube of side {inst.n}")
         self.psis = list(psis)
-        if active is not None:
-            self.active = np.asarray(active, np.int32).copy()
+        if active is None:
+            # every instance that has a state is active
+            active = [1 if (p is not None and inst is not None) else 0
+                      for p, inst in zip(psis, self.instances)]
+        self.active = np.asarray(active, np.int32).copy()
         ptrs = (ctypes.c_void_p * len(psis))(*[p.data_ptr() if p is not None else None for p in psis])
         act = self.active.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         _lib.check(self.lib.gpe_batch_bind(self._h, ptrs, act, _stream()))

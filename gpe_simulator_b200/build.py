@@ -18,8 +18,9 @@ INCLUDE = PKG.parent / "include"
 LIB = PKG / "libgpe_ssf.so"
 OBJ = PKG / "_build"
 
-SOURCES = ["gpe_ssf.cu", "gpe_sweep_f32.cu", "gpe_sweep_f64.cu", "gpe_fast_f32.cu", "gpe_fast_f64.cu",
-           "gpe_noalloc.cu"]
+FAST_SIZES = (32, 48, 64, 96, 128, 160, 256)
+SOURCES = (["gpe_ssf.cu", "gpe_sweep_f32.cu", "gpe_sweep_f64.cu", "gpe_noalloc.cu", "gpe_fast_dispatch.cu"]
+           + [f"gpe_fast_{p}_{n}.cu" for p in ("f32", "f64") for n in FAST_SIZES])
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(INCLUDE),
          "--expt-relaxed-constexpr"]

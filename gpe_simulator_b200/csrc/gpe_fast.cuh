@@ -1,4 +1,4 @@
-// gpe_fast.cuh -- register-resident sweep kernels for N = 64, 128, 256 (sm_100a).
+// gpe_fast.cuh -- register-resident sweep kernels for N = 32, 64, 128, 256 (sm_100a).
 //
 // A line of length N = N1*N2 is transformed in two register phases with one
 // shared-memory exchange between them (the "four-step" split):
@@ -23,15 +23,33 @@
 
 namespace gpe {
 
+// N = N1*N2: phase 1 runs DFT_N2 on N1 lanes, phase 2 DFT_N1 on N2 lanes.
 template <int N> struct Split;
+template <> struct Split<32>  { static constexpr int N1 = 4,  N2 = 8;  };
+template <> struct Split<48>  { static constexpr int N1 = 6,  N2 = 8;  };
 template <> struct Split<64>  { static constexpr int N1 = 8,  N2 = 8;  };
+template <> struct Split<96>  { static constexpr int N1 = 12, N2 = 8;  };
 template <> struct Split<128> { static constexpr int N1 = 8,  N2 = 16; };
+template <> struct Split<160> { static constexpr int N1 = 10, N2 = 16; };
 template <> struct Split<256> { static constexpr int N1 = 16, N2 = 16; };
+template <> struct Split<512> { static constexpr int N1 = 32, N2 = 16; };
 
-// Lines per tile and threads per block of the fast sweeps (elements per thread = L*N/T).
+__host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// Lines per tile L (128-byte rows for y/x tiles; 64-byte for 512) and threads per
+// block T.  The layout (N1 lanes, N2 values) has P1 = L*N1 slots, (N2 lanes, N1
+// values) has P2 = L*N2; a thread holds Q1 (resp. Q2) slots, some threads idle in
+// one phase when P1 != P2 do not divide evenly.
 template <int N, typename R> struct FastCfg {
-  static constexpr int L = sizeof(R) == 4 ? 16 : 8;  // 128-byte rows for P tiles
-  static constexpr int T = L * N / 16;               // 16 elements per thread
+  static constexpr int L = N == 512 ? 8 : (sizeof(R) == 4 ? 16 : 8);
+  static constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  static constexpr int P1 = L * N1, P2 = L * N2;
+  static constexpr bool POW2 = (N & (N - 1)) == 0 && N <= 256;
+  // power-of-two sizes: 16 values per thread; other sizes: one slot per thread per phase
+  static constexpr int T0 = POW2 ? L * N / 16 : cdiv(P1 > P2 ? P1 : P2, 32) * 32;
+  static constexpr int T = T0 < 32 ? 32 : T0;
+  static constexpr int Q1 = cdiv(P1, T), Q2 = cdiv(P2, T);
+  static constexpr int V = Q1 * N2 > Q2 * N1 ? Q1 * N2 : Q2 * N1;   // registers (complex) per thread
 };
 
 enum : int { FZ = 0, FY = 1, FX = 2 };
@@ -105,20 +123,23 @@ __device__ __forceinline__ void slot(int gs, int per, int& l, int& lane) {
 // One forward FFT of every line of the tile, A = lanes in phase 1 (values A-strided),
 // B = values per lane in phase 1.  In: v[s][b] = x[lane_s + A*b] of line l_s (phase-1
 // slots).  Out: v[s][a] = X[lane_s + B*a] (phase-2 slots with B lanes per line).
-template <int N, int A, int B, int AX, typename R, int S1, int S2>
-__device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[S1 * B], typename Cx<R>::T* ex,
+template <int N, int A, int B, int AX, typename R, int QA, int QB, int V>
+__device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename Cx<R>::T* ex,
                                            const typename Cx<R>::T* tw, const typename Cx<R>::T* twl) {
+  // In: QA slots of (A lanes, B values), slot s holding x[lane + A*b] in v[s*B + b].
+  // Out: QB slots of (B lanes, A values), slot s holding X[lane + B*a] in v[s*A + a].
   // tw/twl: 2-D twiddle table of this split, tw[k2*A + lane] = W_N^(lane*k2) (hi, lo):
-  // consecutive lanes read consecutive entries (no bank conflicts in Z tiles)
+  // consecutive lanes read consecutive entries (no bank conflicts in Z tiles).
   using C = typename Cx<R>::T;
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
-  static_assert(S1 * B == S2 * A, "register count must match between phases");
-  // phase 1: DFT_B over the registers, twiddle W_N^(lane*k2)
+  static_assert(QA * B <= V && QB * A <= V, "register array too small");
 #pragma unroll
-  for (int s = 0; s < S1; ++s) {
+  for (int s = 0; s < QA; ++s) {
+    const int gs = threadIdx.x + s * T;
+    if (QA * T > L * A && gs >= L * A) break;
     int l, lane;
-    slot<AX, L>(threadIdx.x + s * T, A, l, lane);
+    slot<AX, L>(gs, A, l, lane);
     C* x = v + s * B;
     Dft<B>::run(x, tw, twl, N / B);
 #pragma unroll
@@ -136,9 +157,11 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[S1 * B], typen
   __syncthreads();
   // phase 2: lane k2 (< B) gathers Y[.][k2], DFT_A
 #pragma unroll
-  for (int s = 0; s < S2; ++s) {
+  for (int s = 0; s < QB; ++s) {
+    const int gs = threadIdx.x + s * T;
+    if (QB * T > L * B && gs >= L * B) break;
     int l, k2;
-    slot<AX, L>(threadIdx.x + s * T, B, l, k2);
+    slot<AX, L>(gs, B, l, k2);
     C* x = v + s * A;
 #pragma unroll
     for (int n1 = 0; n1 < A; ++n1) {
@@ -310,11 +333,19 @@ __device__ __forceinline__ typename Cx<R>::T fast_kin(const Phys& ph, const Fast
   return out;
 }
 
+// true when slot s of this thread exists in a layout with LANES lanes per line
+template <int N, typename R, int LANES, int SLOTS>
+__device__ __forceinline__ bool slot_ok(int s) {
+  constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
+  return !(SLOTS * T > L * LANES) || (int)threadIdx.x + s * T < L * LANES;
+}
+
 template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT, bool REAL, bool CUT>
 __device__ __forceinline__ void kin_all(typename Cx<R>::T (&v)[EPT], const Phys& ph, const FastTables<R>& tb) {
   constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) {
+    if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
     int l, lane;
     slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
 #pragma unroll
@@ -331,11 +362,13 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
                                          const Phys& ph, const FastTables<R>& tb, const R* ctab,
                                          R beta, R h) {
   constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
-  R phs[EPT];
-  R gam[ARR ? EPT : 1];
+  constexpr int E = SLOTS * VALS;
+  R phs[E];
+  R gam[ARR ? E : 1];
   bool small = true;
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) {
+    if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
     int l, lane;
     slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
     const long long row = tl.base + (long long)l * tl.lstride;
@@ -353,50 +386,45 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
       small = small && fabs(phs[e]) <= (REAL ? (R)0.78539816 : (R)0.5);
     }
   }
-  if (sizeof(R) == 8) {
-    // complex128: library exp / sincos in FP64 (the reference's arithmetic)
 #pragma unroll
-    for (int e = 0; e < EPT; ++e) {
-      const typename Cx<R>::T x = v[e];
-      if (!REAL) {
-        const double f = exp(-(double)phs[e]);
-        v[e] = mk((R)(x.x * f), (R)(x.y * f));
-      } else {
-        double sd, cd;
-        sincos((double)phs[e], &sd, &cd);
-        if (ARR) { const double am = exp((double)gam[e]); sd *= am; cd *= am; }
-        v[e] = mk((R)(x.x * cd + x.y * sd), (R)(x.y * cd - x.x * sd));
-      }
-    }
-    return;
-  }
-  if (small) {
+  for (int s = 0; s < SLOTS; ++s) {
+    if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
 #pragma unroll
-    for (int e = 0; e < EPT; ++e) {
+    for (int a = 0; a < VALS; ++a) {
+      const int e = s * VALS + a;
       const typename Cx<R>::T x = v[e];
-      if (!REAL) {
-        const float em = expm1_series((float)-phs[e]);
-        v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
+      if (sizeof(R) == 8) {
+        // complex128: library exp / sincos in FP64 (the reference's arithmetic)
+        if (!REAL) {
+          const double f = exp(-(double)phs[e]);
+          v[e] = mk((R)(x.x * f), (R)(x.y * f));
+        } else {
+          double sd, cd;
+          sincos((double)phs[e], &sd, &cd);
+          if (ARR) { const double am = exp((double)gam[e]); sd *= am; cd *= am; }
+          v[e] = mk((R)(x.x * cd + x.y * sd), (R)(x.y * cd - x.x * sd));
+        }
+      } else if (small) {
+        if (!REAL) {
+          const float em = expm1_series((float)-phs[e]);
+          v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
+        } else {
+          float sn, cm1;
+          sin_cosm1_series((float)phs[e], sn, cm1);
+          if (ARR) { const float am = expm1f((float)gam[e]); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
+          v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
+        }
       } else {
-        float sn, cm1;
-        sin_cosm1_series((float)phs[e], sn, cm1);
-        if (ARR) { const float am = expm1f((float)gam[e]); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
-        v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
-      }
-    }
-  } else {
-#pragma unroll
-    for (int e = 0; e < EPT; ++e) {
-      const typename Cx<R>::T x = v[e];
-      if (!REAL) {
-        const float em = expm1f((float)-phs[e]);
-        v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
-      } else {
-        float sh, ch;
-        sincosf(0.5f * (float)phs[e], &sh, &ch);
-        float cm1 = -2.0f * sh * sh, sn = 2.0f * sh * ch;
-        if (ARR) { const float am = expm1f((float)gam[e]); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
-        v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
+        if (!REAL) {
+          const float em = expm1f((float)-phs[e]);
+          v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
+        } else {
+          float sh, ch;
+          sincosf(0.5f * (float)phs[e], &sh, &ch);
+          float cm1 = -2.0f * sh * sh, sn = 2.0f * sh * ch;
+          if (ARR) { const float am = expm1f((float)gam[e]); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
+          v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
+        }
       }
     }
   }
@@ -447,7 +475,14 @@ __device__ __forceinline__ void fast_pointwise(typename Cx<R>::T (&v)[EPT], cons
   if (MODE == FM_Z21) half_dispatch<N, AX, R, LANES, VALS, SLOTS, EPT>(v, tl, ph, tb, tb.c2);
   if (MODE == FM_Z2 && op.norm) {
 #pragma unroll
-    for (int e = 0; e < EPT; ++e) cx.acc[0].add((double)v[e].x * v[e].x + (double)v[e].y * v[e].y);
+    for (int s = 0; s < SLOTS; ++s) {
+      if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
+#pragma unroll
+      for (int a = 0; a < VALS; ++a) {
+        const typename Cx<R>::T x = v[s * VALS + a];
+        cx.acc[0].add((double)x.x * x.x + (double)x.y * x.y);
+      }
+    }
   }
 }
 
@@ -459,6 +494,7 @@ __device__ __forceinline__ void fast_load(typename Cx<R>::T (&v)[EPT], const Fas
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
 #pragma unroll
   for (int s = 0; s < S1; ++s) {
+    if (!slot_ok<N, R, N1, S1>(s)) break;
     int l, lane;
     slot<AX, L>(threadIdx.x + s * T, N1, l, lane);
 #pragma unroll
@@ -475,6 +511,7 @@ __device__ __forceinline__ void fast_store(const typename Cx<R>::T (&v)[EPT], co
   constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) {
+    if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
     int l, lane;
     slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
 #pragma unroll
@@ -497,9 +534,9 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
-  constexpr int EPT = L * N / T;
-  constexpr int S1 = EPT / N2;
-  constexpr int S2 = EPT / N1;
+  constexpr int EPT = FastCfg<N, R>::V;   // registers (complex) per thread
+  constexpr int S1 = FastCfg<N, R>::Q1;   // slots in layout (N1 lanes, N2 values)
+  constexpr int S2 = FastCfg<N, R>::Q2;   // slots in layout (N2 lanes, N1 values)
   constexpr bool ZM = MODE == FM_Z1 || MODE == FM_Z2 || MODE == FM_Z21;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = (C*)smem_raw;
@@ -525,12 +562,12 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
     const C* gl = (const C*)sw.tw_lo;
     for (int q = threadIdx.x; q < N; q += T) {
       const int k2 = q / N1, n1 = q % N1;   // t1[k2*N1 + n1] = W^(n1*k2)
-      t1[q] = g[(n1 * k2) & (N - 1)];
-      t1l[q] = gl[(n1 * k2) & (N - 1)];
+      t1[q] = g[n1 * k2];                 // n1*k2 < N
+      t1l[q] = gl[n1 * k2];
       if (N1 != N2) {
         const int k2b = q / N2, n2 = q % N2;  // t2[k1*N2 + n2] = W^(n2*k1)
-        t2[q] = g[(n2 * k2b) & (N - 1)];
-        t2l[q] = gl[(n2 * k2b) & (N - 1)];
+        t2[q] = g[n2 * k2b];
+        t2l[q] = gl[n2 * k2b];
       }
     }
   }
@@ -549,12 +586,12 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   fast_load<N, AX, R, S1>(v, tl, (const C*)sw.src, MODE == FM_Z2 || MODE == FM_Z21 || (MODE == FM_PLAIN && op.inv1));
   __syncthreads();  // twiddles and tables visible
   if (MODE == FM_Z1) fast_pointwise<N, AX, R, MODE, 0, N1, N2, S1>(v, tl, ph, tb, op, cx);
-  fft_2phase<N, N1, N2, AX, R, S1, S2>(v, ex, t1, t1l);
+  fft_2phase<N, N1, N2, AX, R, S1, S2, EPT>(v, ex, t1, t1l);
   if (MODE == FM_Z21 || MODE == FM_XKIN) {
     if (MODE == FM_Z21) conj_all(v);  // finish the inverse before the physics
     fast_pointwise<N, AX, R, MODE, 1, N2, N1, S2>(v, tl, ph, tb, op, cx);
     if (MODE == FM_XKIN) conj_all(v);  // start the inverse
-    fft_2phase<N, N2, N1, AX, R, S2, S1>(v, ex, t2, t2l);
+    fft_2phase<N, N2, N1, AX, R, S2, S1, EPT>(v, ex, t2, t2l);
     if (MODE == FM_XKIN) conj_all(v);
     fast_store<N, AX, R, N1, N2, S1>(v, tl, (C*)sw.dst);
   } else {

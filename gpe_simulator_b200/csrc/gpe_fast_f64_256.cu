@@ -1,0 +1,6 @@
+// Register-resident sweeps, n = 256, double.
+#include "gpe_fast_impl.cuh"
+template cudaError_t gpe::launch_fast_n<256, double>(int, const gpe::Phys&, const gpe::Sweep&,
+                                                 const gpe::FastOps&, cudaStream_t);
+template cudaError_t gpe::launch_fastb_n<256, double>(int, const gpe::Phys*, const gpe::Sweep*, int,
+                                                  const gpe::FastOps&, cudaStream_t);

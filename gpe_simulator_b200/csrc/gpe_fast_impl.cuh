@@ -25,7 +25,7 @@ static cudaError_t launch_fast_one(const Phys& ph, const Sweep& sw, const FastOp
 }
 
 template <int N, typename R>
-static cudaError_t launch_fast_n(int ax, const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st) {
+cudaError_t launch_fast_n(int ax, const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st) {
   switch (op.mode) {
     case FM_Z1: return launch_fast_one<N, FZ, R, FM_Z1>(ph, sw, op, st);
     case FM_Z2: return launch_fast_one<N, FZ, R, FM_Z2>(ph, sw, op, st);
@@ -59,7 +59,7 @@ static cudaError_t launch_fastb_one(const Phys* phs, const Sweep* sws, int count
 }
 
 template <int N, typename R>
-static cudaError_t launch_fastb_n(int ax, const Phys* phs, const Sweep* sws, int count, const FastOps& op,
+cudaError_t launch_fastb_n(int ax, const Phys* phs, const Sweep* sws, int count, const FastOps& op,
                                   cudaStream_t st) {
   switch (op.mode) {
     case FM_Z1: return launch_fastb_one<N, FZ, R, FM_Z1>(phs, sws, count, op, st);
@@ -71,27 +71,6 @@ static cudaError_t launch_fastb_n(int ax, const Phys* phs, const Sweep* sws, int
   if (ax == FZ) return launch_fastb_one<N, FZ, R, FM_PLAIN>(phs, sws, count, op, st);
   if (ax == FY) return launch_fastb_one<N, FY, R, FM_PLAIN>(phs, sws, count, op, st);
   return launch_fastb_one<N, FX, R, FM_PLAIN>(phs, sws, count, op, st);
-}
-
-template <typename R>
-cudaError_t launch_fast_batch(int n, int ax, const Phys* phs, const Sweep* sws, int count, const FastOps& op,
-                              cudaStream_t st) {
-  switch (n) {
-    case 64: return launch_fastb_n<64, R>(ax, phs, sws, count, op, st);
-    case 128: return launch_fastb_n<128, R>(ax, phs, sws, count, op, st);
-    case 256: return launch_fastb_n<256, R>(ax, phs, sws, count, op, st);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-template <typename R>
-cudaError_t launch_fast(int n, int ax, const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st) {
-  switch (n) {
-    case 64: return launch_fast_n<64, R>(ax, ph, sw, op, st);
-    case 128: return launch_fast_n<128, R>(ax, ph, sw, op, st);
-    case 256: return launch_fast_n<256, R>(ax, ph, sw, op, st);
-    default: return cudaErrorInvalidValue;
-  }
 }
 
 }  // namespace gpe

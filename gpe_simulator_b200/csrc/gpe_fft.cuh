@@ -18,6 +18,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <type_traits>
 
 namespace gpe {
 
@@ -197,8 +198,99 @@ template <int R1, int R2> struct DftSplit {
   }
 };
 
+// ---- compile-time roots for composite radices other than 8 and 16
+// cos and sin of 2 pi e / rr evaluated at compile time: exact quadrant and
+// half-quadrant reduction in integers, then Taylor series to x^23 on |t| <= pi/4.
+__host__ __device__ constexpr double cx_taylor_sin(double x) {
+  double t = x, s = x;
+  for (int k = 1; k < 12; ++k) { t *= -x * x / ((2.0 * k) * (2.0 * k + 1.0)); s += t; }
+  return s;
+}
+__host__ __device__ constexpr double cx_taylor_cos(double x) {
+  double t = 1.0, s = 1.0;
+  for (int k = 1; k < 12; ++k) { t *= -x * x / ((2.0 * k - 1.0) * (2.0 * k)); s += t; }
+  return s;
+}
+struct CxCS { double c, s; };
+__host__ __device__ constexpr CxCS cx_root(int e, int rr) {
+  const double half_pi = 1.57079632679489661923;
+  e = ((e % rr) + rr) % rr;
+  const int q = (4 * e) / rr, r = 4 * e - q * rr;
+  double cc = 0.0, ss = 0.0;
+  if (2 * r <= rr) {
+    const double t = half_pi * r / rr;
+    cc = cx_taylor_cos(t); ss = cx_taylor_sin(t);
+  } else {
+    const double t = half_pi * (rr - r) / rr;
+    cc = cx_taylor_sin(t); ss = cx_taylor_cos(t);
+  }
+  if (q == 0) return CxCS{cc, ss};
+  if (q == 1) return CxCS{-ss, cc};
+  if (q == 2) return CxCS{-cc, -ss};
+  return CxCS{ss, -cc};
+}
+
+// v * W_RR^E, W_RR = exp(-2 pi i / RR); constants split hi + lo for complex64
+template <int RR, int E, typename C> __device__ __forceinline__ C mul_root(C v) {
+  using R = decltype(v.x);
+  constexpr int e = ((E % RR) + RR) % RR;
+  if constexpr (e == 0) {
+    return v;
+  } else if constexpr (4 * e == RR) {
+    return cmi(v);
+  } else if constexpr (2 * e == RR) {
+    return mk(-v.x, -v.y);
+  } else if constexpr (4 * e == 3 * RR) {
+    return mk(-v.y, v.x);
+  } else {
+    constexpr CxCS w = cx_root(e, RR);
+    constexpr R ch = (R)w.c, sh = (R)w.s;
+    constexpr R cl = (R)(w.c - (double)ch), sl = (R)(w.s - (double)sh);
+    return rot(v, ch, cl, sh, sl);
+  }
+}
+
+template <int B, int E> struct SFor {
+  template <typename F> __device__ __forceinline__ static void run(F&& f) {
+    if constexpr (B < E) {
+      f(std::integral_constant<int, B>{});
+      SFor<B + 1, E>::run(f);
+    }
+  }
+};
+
+// R = R1*R2 from two smaller DFTs with compile-time twiddles W_R^(n2 k1).
+template <int R1, int R2> struct DftSplitG {
+  template <typename C> __device__ __forceinline__ static void run(C* v, const C* tw, const C* twl, int unused) {
+    C y[R2][R1];
+    SFor<0, R2>::run([&](auto n2c) {
+      constexpr int n2 = decltype(n2c)::value;
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) y[n2][n1] = v[R2 * n1 + n2];
+      Dft<R1>::run(y[n2], tw, twl, unused);
+      SFor<1, R1>::run([&](auto k1c) {
+        constexpr int k1 = decltype(k1c)::value;
+        y[n2][k1] = mul_root<R1 * R2, n2 * k1>(y[n2][k1]);
+      });
+    });
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      C z[R2];
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) z[n2] = y[n2][k1];
+      Dft<R2>::run(z, tw, twl, unused);
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = z[k2];
+    }
+  }
+};
+
 template <> struct Dft<8>  : DftSplit<4, 2> {};
 template <> struct Dft<16> : DftSplit<4, 4> {};
+template <> struct Dft<6>  : DftSplitG<3, 2> {};
+template <> struct Dft<10> : DftSplitG<5, 2> {};
+template <> struct Dft<12> : DftSplitG<4, 3> {};
+template <> struct Dft<32> : DftSplitG<4, 8> {};
 
 // Generic odd prime radix (7, 11, 13): direct O(R^2) DFT, W_R^e read from the
 // length-n twiddle table (tw[j] = W_n^j) at stride n/R.

@@ -11,6 +11,7 @@ cudaError_t launch_fast_batch(int n, int ax, const Phys* phs, const Sweep* sws, 
                               cudaStream_t st);
 }
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -181,6 +182,28 @@ __global__ void k_finish_diag(const double* pa, int na, const double* pb, int nb
   }
 }
 
+// Batched finish: block b sums the partials of instance jobs[b] into out[4*index].
+struct DiagJob {
+  const double* pa;
+  const double* pb;
+  int na, nb, index;
+};
+
+__global__ void k_finish_diag_batch(const DiagJob* jobs, double* out) {
+  __shared__ Acc sh[32 * 4];
+  const DiagJob j = jobs[blockIdx.x];
+  Acc a[4];
+  for (int b = threadIdx.x; b < j.na; b += blockDim.x) {
+    a[0].add(j.pa[b * 4 + 0]);
+    a[1].add(j.pa[b * 4 + 1]);
+    a[2].add(j.pa[b * 4 + 2]);
+  }
+  for (int b = threadIdx.x; b < j.nb; b += blockDim.x) a[3].add(j.pb[b * 4 + 3]);
+  block_merge<4>(a, sh);
+  if (threadIdx.x == 0)
+    for (int v = 0; v < 4; ++v) out[4 * j.index + v] = a[v].value();
+}
+
 }  // namespace gpe
 
 // ---------------------------------------------------------------- the plan
@@ -194,7 +217,7 @@ struct gpe_plan {
   Phys ph{};
   int lt_z = 1, lt_yx = 16;
   bool gen = false;                // grid size needs the odd-prime radices 7/11/13
-  bool fast = false;               // register-resident sweeps exist for this n (64, 128, 256)
+  bool fast = false;               // register-resident sweeps exist for this n
   int ept = 16;                    // elements per thread of the sweep family
   int nbins = 0;
   double shell_w = 0;
@@ -404,8 +427,9 @@ int fill_plan(gpe_plan* p, const gpe_desc* d) {
   for (int q = 0; q < p->pp.npass; ++q)
     if (p->pp.radix[q] > 5 && p->pp.radix[q] != 8 && p->pp.radix[q] != 16) p->gen = true;
   p->ept = p->gen ? 8 : 16;
-  // register-resident sweeps: n = 64, 128, 256; potentials from tables (no per-point program)
-  p->fast = (n == 64 || n == 128 || n == 256) && !d->generic_only && d->dynamic_g_len == 0;
+  // register-resident sweeps: n = 32, 48, 64, 96, 128, 160, 256; potentials from tables (no per-point program)
+  p->fast = (n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 160 || n == 256) && !d->generic_only &&
+            d->dynamic_g_len == 0;
   const int emax = 512 * p->ept;
   p->lt_yx = std::max(1, std::min(d->dtype == GPE_C64 ? 16 : 8, emax / n));
   p->lt_z = std::max(1, std::min(n * n, std::min(4096, emax) / n));
@@ -935,6 +959,7 @@ struct gpe_batch {
     int cap = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
+    int uploaded = 0;           // member count the device arrays hold
   };
   std::vector<Group> groups;
   std::vector<void*> psis;
@@ -945,11 +970,15 @@ struct gpe_batch {
   cudaEvent_t ready = nullptr;
   double* h_sums = nullptr;     // pinned, 4 doubles per instance
   long long launches = 0;
+  std::vector<gpe_plan*> parked;  // removed instances awaiting a bulk free
+  DiagJob* d_jobs = nullptr;      // finish jobs of the bound instances
+  double* d_sums = nullptr;       // 4 doubles per instance
+  int jobs = 0, jobs_cap = 0, sums_cap = 0;
 };
 
 namespace {
 
-enum { ROLE_Z1N = 0, ROLE_Z1, ROLE_Y1, ROLE_X, ROLE_Y2, ROLE_Z2, ROLE_SC, ROLE_COUNT };
+enum { ROLE_Z1N = 0, ROLE_Z1, ROLE_Y1, ROLE_X, ROLE_Y2, ROLE_Z2, ROLE_SC, ROLE_DZ, ROLE_DY, ROLE_DX, ROLE_COUNT };
 
 void batch_free_graph(gpe_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
@@ -970,7 +999,11 @@ void batch_free(gpe_batch* b) {
   if (b->ready) cudaEventDestroy(b->ready);
   if (b->cap) cudaStreamDestroy(b->cap);
   if (b->h_sums) cudaFreeHost(b->h_sums);
-  for (auto* p : b->plans) free_plan(p);
+  if (b->d_jobs) cudaFree(b->d_jobs);
+  if (b->d_sums) cudaFree(b->d_sums);
+  for (auto* p : b->plans)
+    if (p) free_plan(p);
+  for (auto* p : b->parked) free_plan(p);
   delete b;
 }
 
@@ -985,14 +1018,21 @@ Sweep role_sweep(int role, void* psi, gpe_plan* p) {
     case ROLE_X: s.fft1 = 1; s.mid = PW_KIN | PW_CONJ_LAST; s.fft2 = 1; s.post = PW_CONJ_FIRST; break;
     case ROLE_Y2: s.pre = PW_CONJ_LAST; s.fft1 = 1; s.post = PW_CONJ_FIRST; break;
     case ROLE_Z2: s.pre = PW_CONJ_LAST; s.fft1 = 1; s.post = PW_CONJ_FIRST | PW_INVM | PW_HALF1 | PW_NORM; break;
-    default: s.pre = PW_SCALE; break;
+    case ROLE_SC: s.pre = PW_SCALE; break;
+    // diagnostics: real-space sums + forward z/y into the work buffer, k-space sums in x
+    case ROLE_DZ: s.dst = p->d_work; s.pre = PW_DIAG_R; s.fft1 = 1; s.t1 = 0.0; break;
+    case ROLE_DY: s.src = p->d_work; s.dst = p->d_work; s.fft1 = 1; break;
+    default:
+      s.src = p->d_work; s.dst = nullptr; s.fft1 = 1; s.post = PW_DIAG_K;
+      s.partial = p->d_partial + 4 * (size_t)p->max_tiles; s.hist = p->d_hist;
+      break;
   }
   return s;
 }
 
 int role_axis(int role) {
-  if (role == ROLE_Y1 || role == ROLE_Y2) return AX_Y;
-  if (role == ROLE_X) return AX_X;
+  if (role == ROLE_Y1 || role == ROLE_Y2 || role == ROLE_DY) return AX_Y;
+  if (role == ROLE_X || role == ROLE_DX) return AX_X;
   return AX_Z;
 }
 
@@ -1000,9 +1040,10 @@ template <typename R>
 int group_launch(gpe_batch* b, gpe_batch::Group& g, int role, cudaStream_t st) {
   const int count = (int)g.members.size();
   if (!count) return GPE_OK;
+  if (g.uploaded != count) return fail(GPE_ERR_ARG, "batch membership changed without gpe_batch_bind");
   const Sweep* sws = g.d_sw + (size_t)role * count;
   const int ax = role_axis(role);
-  if (g.fast && role != ROLE_SC) {
+  if (g.fast && role < ROLE_SC) {
     FastOps op = mk_ops(FM_PLAIN);
     const int fax = ax == AX_Z ? FZ : ax == AX_Y ? FY : FX;
     switch (role) {
@@ -1051,15 +1092,88 @@ int batch_step_all(gpe_batch* b, bool scaled, cudaStream_t st) {
   return GPE_OK;
 }
 
+// Upload the per-instance structs of a group's members (layout [role][member]);
+// `uploaded` records the member count the device arrays were built for.
+int group_upload(gpe_batch* b, gpe_batch::Group& g) {
+  const int m = (int)g.members.size();
+  g.uploaded = m;
+  if (!m) return GPE_OK;
+  if (m > g.cap) {
+    if (g.d_ph) cudaFree(g.d_ph);
+    if (g.d_sw) cudaFree(g.d_sw);
+    g.d_ph = nullptr;
+    g.d_sw = nullptr;
+    CU(cudaMalloc(&g.d_ph, sizeof(Phys) * m));
+    CU(cudaMalloc(&g.d_sw, sizeof(Sweep) * m * ROLE_COUNT));
+    g.cap = m;
+  }
+  std::vector<Phys> hph(m);
+  std::vector<Sweep> hsw((size_t)m * ROLE_COUNT);
+  for (int q = 0; q < m; ++q) {
+    gpe_plan* p = b->plans[g.members[q]];
+    TRY(ensure_work(p));
+    TRY(ensure_hist(p));
+    hph[q] = p->ph;
+    for (int role = 0; role < ROLE_COUNT; ++role) {
+      Sweep s = role_sweep(role, b->psis[g.members[q]], p);
+      int tiles = 0, threads = 0;
+      size_t smem = 0;
+      const int rc = b->dtype == GPE_C64 ? sweep_geometry<float>(p, role_axis(role), s, tiles, threads, smem)
+                                         : sweep_geometry<double>(p, role_axis(role), s, tiles, threads, smem);
+      if (rc != GPE_OK) return rc;
+      hsw[(size_t)role * m + q] = s;
+    }
+  }
+  CU(cudaMemcpyAsync(g.d_ph, hph.data(), sizeof(Phys) * m, cudaMemcpyHostToDevice, g.stream));
+  CU(cudaMemcpyAsync(g.d_sw, hsw.data(), sizeof(Sweep) * m * ROLE_COUNT, cudaMemcpyHostToDevice, g.stream));
+  CU(cudaStreamSynchronize(g.stream));
+  return GPE_OK;
+}
+
+// Finish jobs (one per bound instance) and the device sums array.
+int jobs_upload(gpe_batch* b) {
+  std::vector<DiagJob> jobs;
+  for (auto& g : b->groups)
+    for (int i : g.members) {
+      const gpe_plan* p = b->plans[i];
+      DiagJob j;
+      j.pa = p->d_partial;
+      j.pb = p->d_partial + 4 * (size_t)p->max_tiles;
+      j.na = tiles_of(p, AX_Z);
+      j.nb = tiles_of(p, AX_X);
+      j.index = i;
+      jobs.push_back(j);
+    }
+  b->jobs = (int)jobs.size();
+  if (b->jobs > b->jobs_cap) {
+    if (b->d_jobs) cudaFree(b->d_jobs);
+    b->d_jobs = nullptr;
+    CU(cudaMalloc(&b->d_jobs, sizeof(DiagJob) * b->jobs));
+    b->jobs_cap = b->jobs;
+  }
+  const int n = (int)b->plans.size();
+  if (n > b->sums_cap) {
+    if (b->d_sums) cudaFree(b->d_sums);
+    b->d_sums = nullptr;
+    CU(cudaMalloc(&b->d_sums, sizeof(double) * 4 * n));
+    b->sums_cap = n;
+  }
+  if (b->jobs) {
+    CU(cudaMemcpyAsync(b->d_jobs, jobs.data(), sizeof(DiagJob) * b->jobs, cudaMemcpyHostToDevice, b->cap));
+    CU(cudaStreamSynchronize(b->cap));
+  }
+  return GPE_OK;
+}
+
 }  // namespace
 
 extern "C" {
 
 int gpe_batch_create(const gpe_desc* descs, int count, gpe_batch** out) {
-  if (!descs || !out || count <= 0) return fail(GPE_ERR_ARG, "descs, count > 0 and out are required");
+  if (!out || count < 0 || (count > 0 && !descs)) return fail(GPE_ERR_ARG, "descs (count >= 0) and out are required");
   *out = nullptr;
   gpe_batch* b = new gpe_batch();
-  b->dtype = descs[0].dtype;
+  b->dtype = count > 0 ? descs[0].dtype : GPE_C64;
   for (int i = 0; i < count; ++i) {
     if (descs[i].kind != GPE_IMAGINARY) { batch_free(b); return fail(GPE_ERR_ARG, "batches hold imaginary-time solves"); }
     if (descs[i].dtype != b->dtype) { batch_free(b); return fail(GPE_ERR_ARG, "all instances of a batch share one dtype"); }
@@ -1086,9 +1200,74 @@ int gpe_batch_create(const gpe_desc* descs, int count, gpe_batch** out) {
   CU(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&b->ready, cudaEventDisableTiming));
   CU(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
-  CU(cudaMallocHost(&b->h_sums, sizeof(double) * 4 * count));
+  CU(cudaMallocHost(&b->h_sums, sizeof(double) * 4 * (count > 0 ? count : 1)));
   b->psis.assign(count, nullptr);
   *out = b;
+  return GPE_OK;
+}
+
+int gpe_batch_add(gpe_batch* b, const gpe_desc* d, int* index) {
+  if (!b || !d || !index) return fail(GPE_ERR_ARG, "null argument");
+  if (d->kind != GPE_IMAGINARY) return fail(GPE_ERR_ARG, "batches hold imaginary-time solves");
+  if (d->dtype != b->dtype) return fail(GPE_ERR_ARG, "all instances of a batch share one dtype");
+  gpe_plan* p = nullptr;
+  TRY(create(d, &p));
+  int slot = -1;
+  for (size_t i = 0; i < b->plans.size(); ++i)
+    if (!b->plans[i]) { slot = (int)i; break; }
+  if (slot < 0) {
+    slot = (int)b->plans.size();
+    b->plans.push_back(nullptr);
+    b->psis.push_back(nullptr);
+    double* h = nullptr;
+    CU(cudaMallocHost(&h, sizeof(double) * 4 * b->plans.size()));
+    if (b->h_sums) cudaFreeHost(b->h_sums);
+    b->h_sums = h;
+  }
+  b->plans[slot] = p;
+  b->psis[slot] = nullptr;
+  int gi = -1;
+  for (size_t q = 0; q < b->groups.size(); ++q)
+    if (b->groups[q].n == p->n) gi = (int)q;
+  if (gi < 0) {
+    gpe_batch::Group g;
+    g.n = p->n;
+    g.fast = p->fast;
+    CU(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+    CU(cudaEventCreateWithFlags(&g.ev, cudaEventDisableTiming));
+    b->groups.push_back(g);
+    gi = (int)b->groups.size() - 1;
+  }
+  b->groups[gi].all.push_back(slot);
+  *index = slot;
+  return GPE_OK;
+}
+
+// Removal requires the batch's work to be finished: call it after a synchronising
+// call on the batch's stream (gpe_batch_diagnostics) or a stream synchronise.
+int gpe_batch_remove(gpe_batch* b, int index) {
+  if (!b || index < 0 || index >= (int)b->plans.size() || !b->plans[index])
+    return fail(GPE_ERR_ARG, "no such batch instance");
+  // The caller has synchronised the batch's stream (the graph is idle).  Freeing
+  // device memory would wait for every stream of the device, so removed plans are
+  // parked and freed together once enough have accumulated.
+  for (auto& g : b->groups) CU(cudaStreamSynchronize(g.stream));
+  batch_free_graph(b);
+  b->psis[index] = nullptr;
+  for (auto& g : b->groups) {
+    g.all.erase(std::remove(g.all.begin(), g.all.end(), index), g.all.end());
+    const size_t before = g.members.size();
+    g.members.erase(std::remove(g.members.begin(), g.members.end(), index), g.members.end());
+    if (g.members.size() != before) TRY(group_upload(b, g));
+  }
+  TRY(jobs_upload(b));
+  b->parked.push_back(b->plans[index]);
+  if (b->parked.size() >= 64) {
+    for (auto* q : b->parked) free_plan(q);
+    b->parked.clear();
+  }
+  b->plans[index] = nullptr;
+  b->psis[index] = nullptr;
   return GPE_OK;
 }
 
@@ -1105,43 +1284,14 @@ int gpe_batch_bind(gpe_batch* b, void* const* psis, const int* active, void* str
   CU(cudaStreamSynchronize((cudaStream_t)stream));
   for (auto& g : b->groups) CU(cudaStreamSynchronize(g.stream));
   batch_free_graph(b);
-  for (int i = 0; i < count; ++i) b->psis[i] = psis[i];
+  for (int i = 0; i < count; ++i) b->psis[i] = b->plans[i] ? psis[i] : nullptr;
   for (auto& g : b->groups) {
     g.members.clear();
     for (int i : g.all)
-      if ((!active || active[i]) && psis[i]) g.members.push_back(i);
-    const int m = (int)g.members.size();
-    if (!m) continue;
-    if (m > g.cap) {
-      if (g.d_ph) cudaFree(g.d_ph);
-      if (g.d_sw) cudaFree(g.d_sw);
-      g.d_ph = nullptr;
-      g.d_sw = nullptr;
-      CU(cudaMalloc(&g.d_ph, sizeof(Phys) * m));
-      CU(cudaMalloc(&g.d_sw, sizeof(Sweep) * m * ROLE_COUNT));
-      g.cap = m;
-    }
-    std::vector<Phys> hph(m);
-    std::vector<Sweep> hsw((size_t)m * ROLE_COUNT);
-    for (int q = 0; q < m; ++q) {
-      gpe_plan* p = b->plans[g.members[q]];
-      TRY(ensure_work(p));
-      TRY(ensure_hist(p));
-      hph[q] = p->ph;
-      for (int role = 0; role < ROLE_COUNT; ++role) {
-        Sweep s = role_sweep(role, psis[g.members[q]], p);
-        int tiles = 0, threads = 0;
-        size_t smem = 0;
-        const int rc = b->dtype == GPE_C64 ? sweep_geometry<float>(p, role_axis(role), s, tiles, threads, smem)
-                                           : sweep_geometry<double>(p, role_axis(role), s, tiles, threads, smem);
-        if (rc != GPE_OK) return rc;
-        hsw[(size_t)role * m + q] = s;
-      }
-    }
-    CU(cudaMemcpy(g.d_ph, hph.data(), sizeof(Phys) * m, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(g.d_sw, hsw.data(), sizeof(Sweep) * m * ROLE_COUNT, cudaMemcpyHostToDevice));
+      if ((!active || active[i]) && b->psis[i]) g.members.push_back(i);
+    TRY(group_upload(b, g));
   }
-  return GPE_OK;
+  return jobs_upload(b);
 }
 
 int gpe_batch_step(gpe_batch* b, int nsteps, void* stream) {
@@ -1181,26 +1331,25 @@ int gpe_batch_step(gpe_batch* b, int nsteps, void* stream) {
 int gpe_batch_diagnostics(gpe_batch* b, double* scalars, void* stream) {
   if (!b || !scalars) return fail(GPE_ERR_ARG, "null argument");
   cudaStream_t st = (cudaStream_t)stream;
-  const int count = (int)b->plans.size();
-  for (int i = 0; i < count; ++i) {
-    bool bound = false;
-    for (auto& g : b->groups)
-      for (int m : g.members) bound = bound || m == i;
-    if (!bound) continue;
-    gpe_plan* p = b->plans[i];
-    TRY(diag_launch(p, b->psis[i], 0.0, st));
-    k_finish_diag<<<1, 256, 0, st>>>(p->d_partial, tiles_of(p, AX_Z), p->d_partial + 4 * (size_t)p->max_tiles,
-                                     tiles_of(p, AX_X), nullptr, p->nbins, p->d_out);
-    CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(b->h_sums + 4 * i, p->d_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (!b->jobs) return GPE_OK;
+  CU(cudaEventRecord(b->fork, st));
+  for (auto& g : b->groups) {
+    if (g.members.empty()) continue;
+    CU(cudaStreamWaitEvent(g.stream, b->fork, 0));
+    TRY(group_role(b, g, ROLE_DZ, g.stream));
+    TRY(group_role(b, g, ROLE_DY, g.stream));
+    TRY(group_role(b, g, ROLE_DX, g.stream));
+    CU(cudaEventRecord(g.ev, g.stream));
+    CU(cudaStreamWaitEvent(st, g.ev, 0));
   }
+  k_finish_diag_batch<<<b->jobs, 256, 0, st>>>(b->d_jobs, b->d_sums);
+  CU(cudaGetLastError());
+  ++b->launches;
+  const int n = (int)b->plans.size();
+  CU(cudaMemcpyAsync(b->h_sums, b->d_sums, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
-  for (int i = 0; i < count; ++i) {
-    bool bound = false;
-    for (auto& g : b->groups)
-      for (int m : g.members) bound = bound || m == i;
-    if (bound) diag_scalars(b->plans[i], b->h_sums + 4 * i, scalars + 6 * i);
-  }
+  for (auto& g : b->groups)
+    for (int i : g.members) diag_scalars(b->plans[i], b->h_sums + 4 * i, scalars + 6 * i);
   return GPE_OK;
 }
 

@@ -168,6 +168,10 @@ int  gpe_status(gpe_plan* plan, int* flags, void* stream);
  * launch per group over (tiles x instances), and one step of all groups is
  * replayed from a CUDA graph with a parallel branch per group.  Replaces calling
  * standard_imaginary_step (gpe/make_propagator.py:109-151) for each solve in turn.
+ *   gpe_batch_create: count >= 0 instances (an empty batch takes its dtype from
+ *     the first gpe_batch_add when count = 0 -- complex64 otherwise).
+ *   gpe_batch_add / gpe_batch_remove: grow or shrink a running batch (continuous
+ *     batching); add returns the new instance's index (a freed index is reused).
  *   gpe_batch_bind: psi pointers of every instance (device, C-contiguous) and an
  *     optional active mask (NULL = all); rebinding discards the captured graph.
  *   gpe_batch_step: nsteps renormalised steps of every bound instance.
@@ -176,6 +180,8 @@ int  gpe_status(gpe_plan* plan, int* flags, void* stream);
 typedef struct gpe_batch gpe_batch;
 int  gpe_batch_create(const gpe_desc* descs, int count, gpe_batch** batch);
 int  gpe_batch_destroy(gpe_batch* batch);
+int  gpe_batch_add(gpe_batch* batch, const gpe_desc* desc, int* index);
+int  gpe_batch_remove(gpe_batch* batch, int index);
 int  gpe_batch_bind(gpe_batch* batch, void* const* psis, const int* active, void* stream);
 int  gpe_batch_step(gpe_batch* batch, int nsteps, void* stream);
 int  gpe_batch_diagnostics(gpe_batch* batch, double* scalars, void* stream);

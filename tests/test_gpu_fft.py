@@ -6,7 +6,7 @@ import torch
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [2, 4, 7, 8, 12, 16, 18, 30, 48, 64, 96, 128, 160]
+SIZES = [2, 4, 7, 8, 12, 16, 18, 30, 32, 48, 64, 96, 128, 160]
 
 
 def _plan(n, dtype):

@@ -1,4 +1,4 @@
-"""The register-resident sweeps (n = 64, 128, 256) against the generic
+"""The register-resident sweeps (n = 32 ... 256) against the generic
 mixed-radix sweeps and the oracle, for every step sequence they implement."""
 
 import numpy as np
@@ -17,7 +17,7 @@ def make(n, L, kind, dtype, generic, **kw):
     return Plan(n, x, k, dtype=dtype, kind=kind, generic_only=generic, **kw), x
 
 
-@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("n", [32, 48, 64, 96, 128, 160])
 @pytest.mark.parametrize("dtype,tol", [(torch.complex128, 1e-13), (torch.complex64, 3e-6)])
 @pytest.mark.parametrize("kind", ["imaginary", "real"])
 def test_fast_matches_generic_and_oracle(cuda, n, dtype, tol, kind):
@@ -41,7 +41,7 @@ def test_fast_matches_generic_and_oracle(cuda, n, dtype, tol, kind):
     assert err < (1e-12 if dtype == torch.complex128 else 1e-5), err
 
 
-@pytest.mark.parametrize("n", [64, 128, 256])
+@pytest.mark.parametrize("n", [32, 48, 64, 96, 128, 160, 256])
 def test_fast_fft_matches_numpy(cuda, n):
     p, _ = make(n, 10.0, "imaginary", torch.complex64, False, beta=0.0, dt=0.0)
     g = torch.Generator(device="cuda").manual_seed(n)
