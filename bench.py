@@ -37,6 +37,10 @@ METRIC = "steps/s & HBM roofline % at 256^3 c64"
 WORKLOAD = ("stir256_c64: real-time stirred GPE, 256^3 complex64, box [-12,12)^3, g=2000, "
             "dt=2.5e-4, beam A=10 w=0.5 R=2 Omega 0->0.5 over 200 steps")
 FALLBACK_HBM = 6650.0
+# the sweep kernel of each axis in one real-time step (register-resident path, n = 256)
+KERNELS = {"z": "k_fast_occ<256, 0, float, 3, 3> (fused z sweep)",
+           "y": "k_fast_occ<256, 1, float, 0, 4> (y sweep, 2 per step)",
+           "x": "k_fast_occ<256, 2, float, 4, 3> (x sweep with kinetic phase)"}
 
 
 def measured_peak():
@@ -252,7 +256,8 @@ def ours(args, world, rank, local):
                    "l2": "inputs larger than L2 (128 MiB psi vs 126 MB L2), no flush"},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "kernel": f"k_sweep axis {dom}",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": KERNELS[dom],
+                     "traffic_source": "profiles/traffic.json (ncu dram bytes read + write per launch)",
                      "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_per_launch,
                      "avg_launch_ms": dom_ms / dom_n,

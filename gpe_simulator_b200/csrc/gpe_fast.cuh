@@ -68,9 +68,9 @@ struct FastOps {
   int norm;         // FM_Z2: norm partials and renormalisation scale
 };
 
-// per-tile table bytes (kx, kyz, kx2, kyz2, vz, c1, c2), rounded to 16
+// per-tile table bytes (kx, kyz, kx2, kyz2, vz, c1, c2, c12), rounded to 16
 template <int N, typename R> __host__ __device__ constexpr size_t fast_tables_bytes() {
-  return (((size_t)(N + FastCfg<N, R>::L) * (16 + 8) + (size_t)(N + 2 * FastCfg<N, R>::L) * sizeof(R)) + 15)
+  return (((size_t)(N + FastCfg<N, R>::L) * (16 + 8) + (size_t)(N + 3 * FastCfg<N, R>::L) * sizeof(R)) + 15)
          / 16 * 16;
 }
 
@@ -215,54 +215,13 @@ __device__ __forceinline__ float expm1_series(float x) {
   }
 }
 
-// Local half-step factor for a potential value V (reference gpe/make_kernel.py:14-119);
-// gam = Im V_static (real time, 0 if none).  complex64 applies v + v*(f - 1).
-template <typename R>
-__device__ __forceinline__ typename Cx<R>::T fast_local(const Phys& ph, typename Cx<R>::T v, R V, R gam) {
-  if (sizeof(R) == 8 || ph.local_fp64) {
-    const double vx = v.x, vy = v.y, hd = ph.dt * 0.5;
-    const double phd = ((double)V + ph.beta * (vx * vx + vy * vy)) * hd;
-    if (ph.kind == 0) {
-      const double f = exp(-phd);
-      return mk((R)(vx * f), (R)(vy * f));
-    }
-    double sd, cd;
-    sincos(phd, &sd, &cd);
-    if (gam != (R)0) {
-      const double a = exp((double)gam * hd);
-      cd *= a; sd *= a;
-    }
-    return mk((R)(vx * cd + vy * sd), (R)(vy * cd - vx * sd));
-  }
-  const float h = (float)(ph.dt * 0.5);
-  const float phase = ((float)V + (float)ph.beta * (v.x * v.x + v.y * v.y)) * h;
-  if (ph.kind == 0) {
-    const float e = fabsf(phase) <= 0.5f ? expm1_series(-phase) : expm1f(-phase);
-    return mk(fma(v.x, (R)e, v.x), fma(v.y, (R)e, v.y));
-  }
-  float cm1, sn;
-  if (fabsf(phase) <= 0.78539816f) {
-    sin_cosm1_series(phase, sn, cm1);
-  } else {
-    float sh, ch;
-    sincosf(0.5f * phase, &sh, &ch);
-    cm1 = -2.0f * sh * sh;
-    sn = 2.0f * sh * ch;
-  }
-  if (gam != (R)0) {
-    const float am1 = expm1f((float)gam * h);
-    cm1 = am1 + cm1 + am1 * cm1;
-    sn = sn + sn * am1;
-  }
-  return mk(fma(v.x, (R)cm1, fma(v.y, (R)sn, v.x)), fma(v.y, (R)cm1, fma(-v.x, (R)sn, v.y)));
-}
-
 // Per-tile tables in shared memory.
 template <typename R>
 struct FastTables {
   R* vz;          // [N] static potential along z (Z tiles)
   R* c1;          // [L] vx(i) + vy(j_l) + beam(i, j_l; t1)
   R* c2;          // [L] same at t2
+  R* c12;         // [L] c1 + c2
   double2* kx;    // [N] kinetic factors along the transform axis (X tiles)
   double2* kyz;   // [L] kinetic factor of (j, k_l)
   double* kx2;    // [N] k^2 along x (cutoff)
@@ -293,6 +252,7 @@ __device__ __forceinline__ void z_tables(const Phys& ph, const Sweep& sw, int a0
     }
     tb.c1[threadIdx.x] = base + b1;
     tb.c2[threadIdx.x] = base + b2;
+    tb.c12[threadIdx.x] = (base + b1) + (base + b2);
   }
 }
 
@@ -357,7 +317,11 @@ __device__ __forceinline__ void kin_all(typename Cx<R>::T (&v)[EPT], const Phys&
 // LANES*a, Z tiles: m = z index), potential vz[m] + ctab[l] (+ arrays).  The
 // phases are computed first; whether all of this thread's phases lie in the
 // series' range is decided once, so each element loop is straight-line code.
-template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT, bool REAL, bool ARR>
+// TWO: two consecutive real-time half-steps at one point as one rotation by
+// (2 vz[m] + ctab[l] + 2 beta |psi|^2) dt/2 with ctab = c1 + c2; exact because
+// the first rotation leaves |psi| unchanged (callers pass beta already doubled).
+template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT, bool REAL, bool ARR,
+          bool TWO = false>
 __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
                                          const Phys& ph, const FastTables<R>& tb, const R* ctab,
                                          R beta, R h) {
@@ -376,7 +340,7 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
 #pragma unroll
     for (int a = 0; a < VALS; ++a) {
       const int e = s * VALS + a, m = lane + LANES * a;
-      R V = tb.vz[m] + c;
+      R V = TWO ? (R)2 * tb.vz[m] + c : tb.vz[m] + c;
       if (ARR) {
         V += ph.vre ? ((const R*)ph.vre)[row + m] : (R)0;
         gam[e] = ph.vim ? ((const R*)ph.vim)[row + m] * h : (R)0;
@@ -471,6 +435,12 @@ __device__ __forceinline__ void fast_pointwise(typename Cx<R>::T (&v)[EPT], cons
     return;
   }
   scale_all(v, (R)ph.inv_m);
+  if (MODE == FM_Z21 && ph.kind == 1 && ph.vre == nullptr && ph.vim == nullptr) {
+    // real time, potential from tables: the two half-steps as one rotation
+    half_all<N, AX, R, LANES, VALS, SLOTS, EPT, true, false, true>(v, tl, ph, tb, tb.c12, (R)(2.0 * ph.beta),
+                                                                   (R)(ph.dt * 0.5));
+    return;
+  }
   half_dispatch<N, AX, R, LANES, VALS, SLOTS, EPT>(v, tl, ph, tb, tb.c1);
   if (MODE == FM_Z21) half_dispatch<N, AX, R, LANES, VALS, SLOTS, EPT>(v, tl, ph, tb, tb.c2);
   if (MODE == FM_Z2 && op.norm) {
@@ -552,6 +522,7 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   tb.vz = (R*)(tb.kyz2 + L);
   tb.c1 = tb.vz + N;
   tb.c2 = tb.c1 + L;
+  tb.c12 = tb.c2 + L;
   // 2-D twiddle tables: t1 for the split (N1 lanes, N2 values), t2 for (N2, N1)
   C* t1 = tw;
   C* t1l = twl;
@@ -607,15 +578,29 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   }
 }
 
+// Resident blocks per SM that the register allocation must allow, 0 = the
+// compiler's choice.  Measured for complex64 at n = 128, 256: the plain FFT
+// sweeps are memory-bound and want 1024 threads per SM (64 registers at
+// T = 256); the fused modes keep 768 (85 registers) for their extra live state.
+template <int N, typename R, int MODE> struct FastBounds {
+  static constexpr int value = (sizeof(R) == 4 && (N == 128 || N == 256))
+                                   ? (MODE == FM_PLAIN ? 1024 : 768) / FastCfg<N, R>::T : 0;
+};
+
 template <int N, int AX, typename R, int MODE>
 __global__ void __launch_bounds__(FastCfg<N, R>::T) k_fast(Phys ph, Sweep sw, FastOps op) {
   fast_body<N, AX, R, MODE>(ph, sw, op);
 }
 
+template <int N, int AX, typename R, int MODE, int B>
+__global__ void __launch_bounds__(FastCfg<N, R>::T, B) k_fast_occ(Phys ph, Sweep sw, FastOps op) {
+  fast_body<N, AX, R, MODE>(ph, sw, op);
+}
+
 // Batched launch: blockIdx.y selects the instance (structs staged in shared memory).
 template <int N, int AX, typename R, int MODE>
-__global__ void __launch_bounds__(FastCfg<N, R>::T) k_fast_batch(const Phys* __restrict__ phs,
-                                                                const Sweep* __restrict__ sws, FastOps op) {
+__device__ __forceinline__ void fast_batch_body(const Phys* __restrict__ phs, const Sweep* __restrict__ sws,
+                                                const FastOps& op) {
   __shared__ Phys ph;
   __shared__ Sweep sw;
   if (threadIdx.x == 0) {
@@ -624,6 +609,18 @@ __global__ void __launch_bounds__(FastCfg<N, R>::T) k_fast_batch(const Phys* __r
   }
   __syncthreads();
   fast_body<N, AX, R, MODE>(ph, sw, op);
+}
+
+template <int N, int AX, typename R, int MODE>
+__global__ void __launch_bounds__(FastCfg<N, R>::T) k_fast_batch(const Phys* __restrict__ phs,
+                                                                const Sweep* __restrict__ sws, FastOps op) {
+  fast_batch_body<N, AX, R, MODE>(phs, sws, op);
+}
+
+template <int N, int AX, typename R, int MODE, int B>
+__global__ void __launch_bounds__(FastCfg<N, R>::T, B) k_fast_batch_occ(const Phys* __restrict__ phs,
+                                                                       const Sweep* __restrict__ sws, FastOps op) {
+  fast_batch_body<N, AX, R, MODE>(phs, sws, op);
 }
 
 }  // namespace gpe

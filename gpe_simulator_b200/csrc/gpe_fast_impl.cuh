@@ -5,22 +5,34 @@
 
 namespace gpe {
 
+// the kernel of (N, AX, R, MODE): explicit occupancy bounds where measured
+template <int N, int AX, typename R, int MODE> constexpr auto fast_kernel() {
+  constexpr int B = FastBounds<N, R, MODE>::value;
+  if constexpr (B > 0) return &k_fast_occ<N, AX, R, MODE, B>;
+  else return &k_fast<N, AX, R, MODE>;
+}
+template <int N, int AX, typename R, int MODE> constexpr auto fast_batch_kernel() {
+  constexpr int B = FastBounds<N, R, MODE>::value;
+  if constexpr (B > 0) return &k_fast_batch_occ<N, AX, R, MODE, B>;
+  else return &k_fast_batch<N, AX, R, MODE>;
+}
+
 template <int N, int AX, typename R, int MODE>
 static cudaError_t launch_fast_one(const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st) {
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
   const int tiles = AX == FZ ? N * N / L : N * (N / L);
   constexpr size_t smem = fast_smem_bytes<N, R>();
+  constexpr auto kern = fast_kernel<N, AX, R, MODE>();
   static int attr_dev = -1;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
-    cudaError_t e = cudaFuncSetAttribute(k_fast<N, AX, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_dev = dev;
   }
-  k_fast<N, AX, R, MODE><<<tiles, T, smem, st>>>(ph, sw, op);
+  kern<<<tiles, T, smem, st>>>(ph, sw, op);
   return cudaGetLastError();
 }
 
@@ -45,16 +57,16 @@ static cudaError_t launch_fastb_one(const Phys* phs, const Sweep* sws, int count
   constexpr int T = FastCfg<N, R>::T;
   const int tiles = AX == FZ ? N * N / L : N * (N / L);
   constexpr size_t smem = fast_smem_bytes<N, R>();
+  constexpr auto kern = fast_batch_kernel<N, AX, R, MODE>();
   static int attr_dev = -1;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
-    cudaError_t e = cudaFuncSetAttribute(k_fast_batch<N, AX, R, MODE>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_dev = dev;
   }
-  k_fast_batch<N, AX, R, MODE><<<dim3(tiles, count), T, smem, st>>>(phs, sws, op);
+  kern<<<dim3(tiles, count), T, smem, st>>>(phs, sws, op);
   return cudaGetLastError();
 }
 
