@@ -37,10 +37,11 @@ METRIC = "steps/s & HBM roofline % at 256^3 c64"
 WORKLOAD = ("stir256_c64: real-time stirred GPE, 256^3 complex64, box [-12,12)^3, g=2000, "
             "dt=2.5e-4, beam A=10 w=0.5 R=2 Omega 0->0.5 over 200 steps")
 FALLBACK_HBM = 6650.0
-# the sweep kernel of each axis in one real-time step (register-resident path, n = 256)
+# the sweep kernel of each axis in one real-time step at n = 256
 KERNELS = {"z": "k_fast_occ<256, 0, float, 3, 3> (fused z sweep)",
            "y": "k_fast_occ<256, 1, float, 0, 4> (y sweep, 2 per step)",
            "x": "k_fast_occ<256, 2, float, 4, 3> (x sweep with kinetic phase)"}
+TRAFFIC_KEYS = {"z": "sweep_z", "y": "sweep_y", "x": "sweep_x"}
 
 
 def measured_peak():
@@ -214,7 +215,7 @@ def ours(args, world, rank, local):
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(f"sweep_{dom}")
+        traffic = json.loads(tfile.read_text()).get(TRAFFIC_KEYS[dom])
 
     # ---- end to end: public closure API with host buffers, H2D + D2H every step
     from gpe_simulator_b200.make_propagator import make_real_propagator

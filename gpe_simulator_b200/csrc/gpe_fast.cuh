@@ -134,6 +134,10 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
   static_assert(QA * B <= V && QB * A <= V, "register array too small");
+  // Z tiles with A == B lanes per line in both phases and one slot per thread:
+  // every line is owned by the same warp in both phases (32/A lines per warp)
+  // and its exchange rows are its own, so a warp barrier suffices.
+  constexpr bool WARP_LOCAL = AX == FZ && A == B && QA == 1 && QB == 1 && 32 % A == 0 && L * A == T;
 #pragma unroll
   for (int s = 0; s < QA; ++s) {
     const int gs = threadIdx.x + s * T;
@@ -154,7 +158,7 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
       ex[idx] = x[k2];
     }
   }
-  __syncthreads();
+  if (WARP_LOCAL) __syncwarp(); else __syncthreads();
   // phase 2: lane k2 (< B) gathers Y[.][k2], DFT_A
 #pragma unroll
   for (int s = 0; s < QB; ++s) {
@@ -170,7 +174,7 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
     }
     Dft<A>::run(x, tw, twl, N / A);
   }
-  __syncthreads();
+  if (WARP_LOCAL) __syncwarp(); else __syncthreads();
 }
 
 template <typename R>
@@ -456,8 +460,9 @@ __device__ __forceinline__ void fast_pointwise(typename Cx<R>::T (&v)[EPT], cons
   }
 }
 
-// Load the tile into registers in layout (N1 lanes, N2 values).
-template <int N, int AX, typename R, int S1, int EPT>
+// Load the tile into registers in layout (N1 lanes, N2 values); CG: through L2
+// only (data another block wrote during the same launch).
+template <int N, int AX, typename R, int S1, bool CG, int EPT>
 __device__ __forceinline__ void fast_load(typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
                                           const typename Cx<R>::T* __restrict__ src, bool conj) {
   constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
@@ -469,7 +474,7 @@ __device__ __forceinline__ void fast_load(typename Cx<R>::T (&v)[EPT], const Fas
     slot<AX, L>(threadIdx.x + s * T, N1, l, lane);
 #pragma unroll
     for (int b = 0; b < N2; ++b) {
-      const typename Cx<R>::T x = src[tl.gidx(l, lane + N1 * b)];
+      const typename Cx<R>::T x = CG ? __ldcg(src + tl.gidx(l, lane + N1 * b)) : src[tl.gidx(l, lane + N1 * b)];
       v[s * N2 + b] = conj ? conj_<R>(x) : x;
     }
   }
@@ -498,8 +503,9 @@ __device__ __forceinline__ void fast_store(const typename Cx<R>::T (&v)[EPT], co
 //   FM_Z2     inverse, 1/M, half(t1) [norm partials]                last z sweep of a step
 //   FM_Z21    inverse, 1/M, half(t1), half(t2), forward             last z of a step + first z of the next
 //   FM_XKIN   forward, kinetic, inverse                             x sweep
-template <int N, int AX, typename R, int MODE>
-__device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const FastOps& op) {
+template <int N, int AX, typename R, int MODE, bool CG = false>
+__device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const FastOps& op, int tile,
+                                          int ntiles) {
   using C = typename Cx<R>::T;
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
@@ -542,7 +548,7 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
       }
     }
   }
-  const FastTile<N, AX, R> tl(blockIdx.x);
+  const FastTile<N, AX, R> tl(tile);
   if (ZM) z_tables<N, R>(ph, sw, tl.a0, tb, MODE == FM_Z21);
   if (MODE == FM_XKIN) x_tables<N, R>(ph, tl.a0, tl.b0, tb);
   PwCtx<R> cx;
@@ -554,7 +560,7 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   }
 
   C v[EPT];
-  fast_load<N, AX, R, S1>(v, tl, (const C*)sw.src, MODE == FM_Z2 || MODE == FM_Z21 || (MODE == FM_PLAIN && op.inv1));
+  fast_load<N, AX, R, S1, CG>(v, tl, (const C*)sw.src, MODE == FM_Z2 || MODE == FM_Z21 || (MODE == FM_PLAIN && op.inv1));
   __syncthreads();  // twiddles and tables visible
   if (MODE == FM_Z1) fast_pointwise<N, AX, R, MODE, 0, N1, N2, S1>(v, tl, ph, tb, op, cx);
   fft_2phase<N, N1, N2, AX, R, S1, S2, EPT>(v, ex, t1, t1l);
@@ -574,7 +580,7 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   if (MODE == FM_Z2 && op.norm) {
     Acc a[1] = {cx.acc[0]};
     block_merge<1>(a, red);
-    norm_finish(ph, sw, a[0], red);
+    norm_finish_n(ph, sw, a[0], red, tile, ntiles);
   }
 }
 
@@ -589,12 +595,12 @@ template <int N, typename R, int MODE> struct FastBounds {
 
 template <int N, int AX, typename R, int MODE>
 __global__ void __launch_bounds__(FastCfg<N, R>::T) k_fast(Phys ph, Sweep sw, FastOps op) {
-  fast_body<N, AX, R, MODE>(ph, sw, op);
+  fast_body<N, AX, R, MODE>(ph, sw, op, blockIdx.x, gridDim.x);
 }
 
 template <int N, int AX, typename R, int MODE, int B>
 __global__ void __launch_bounds__(FastCfg<N, R>::T, B) k_fast_occ(Phys ph, Sweep sw, FastOps op) {
-  fast_body<N, AX, R, MODE>(ph, sw, op);
+  fast_body<N, AX, R, MODE>(ph, sw, op, blockIdx.x, gridDim.x);
 }
 
 // Batched launch: blockIdx.y selects the instance (structs staged in shared memory).
@@ -608,7 +614,7 @@ __device__ __forceinline__ void fast_batch_body(const Phys* __restrict__ phs, co
     sw = sws[blockIdx.y];
   }
   __syncthreads();
-  fast_body<N, AX, R, MODE>(ph, sw, op);
+  fast_body<N, AX, R, MODE>(ph, sw, op, blockIdx.x, gridDim.x);
 }
 
 template <int N, int AX, typename R, int MODE>
@@ -621,6 +627,115 @@ template <int N, int AX, typename R, int MODE, int B>
 __global__ void __launch_bounds__(FastCfg<N, R>::T, B) k_fast_batch_occ(const Phys* __restrict__ phs,
                                                                        const Sweep* __restrict__ sws, FastOps op) {
   fast_batch_body<N, AX, R, MODE>(phs, sws, op);
+}
+
+
+// ---------------------------------------------------------------- plane-fused sweeps
+// The y and z sweeps of a step never leave an x-plane: a y tile (16 z columns
+// of one plane) needs the whole plane's z sweep, a z tile (16 z lines) the
+// whole plane's y sweep, and nothing else.  One persistent launch runs up to
+// three consecutive y/z sweeps (e.g. inverse y, fused z, forward y) as a task
+// list: task = (plane, stage, tile), handed out by an atomic ticket in an order
+// where every task's dependencies hold smaller tickets (windows of W planes,
+// software-pipelined: stage s of window w runs in block w + s).  A task of
+// stage s > 0 waits (bounded) until the plane's stage s-1 count reaches its
+// tile count; blocks that hold smaller tickets are resident and never wait on
+// larger ones, so the wait always ends.  Intermediate planes stay in L2: psi
+// crosses HBM once in and once out per launch instead of once per sweep.
+struct PlaneJob {
+  FastOps op[3];    // per stage
+  int nstage;       // 1..3
+  int zstage;       // the z stage; the others are y sweeps
+  int window;       // planes per scheduling window (divides N)
+  unsigned* ctr;    // [0] task ticket, [1] blocks finished, [2 + 3p + s] tiles done of (plane p, stage s)
+};
+
+// bounded wait of a plane-fused task (iterations of ~64 ns sleeps, ~0.3 s)
+constexpr int PLANE_WAIT_LIMIT = 1 << 22;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <int N, typename R, int MZ>
+__device__ __forceinline__ void plane_body(const Phys& ph, const Sweep& sw, const PlaneJob& job) {
+  constexpr int L = FastCfg<N, R>::L;
+  constexpr int TPP = N / L;   // tiles per plane and stage
+  static_assert(N % L == 0, "plane tiles");
+  const int ns = job.nstage, W = job.window;
+  const int nw = N / W;   // windows
+  const unsigned per_stage = (unsigned)W * TPP;
+  const unsigned total = (unsigned)N * TPP * ns;
+  unsigned* ticket = job.ctr;
+  unsigned* finished = job.ctr + 1;
+  unsigned* done = job.ctr + 2;
+  // tickets are fetched one task ahead so the atomic's latency hides behind a
+  // task (a held, not yet started task waits on nothing, so the order argument
+  // above still holds)
+  __shared__ unsigned s_task[2];
+  if (threadIdx.x == 0) s_task[0] = atomicAdd(ticket, 1u);
+  for (int k = 0;; k ^= 1) {
+    __syncthreads();  // the previous task is done with shared memory; s_task[k] visible
+    const unsigned t = s_task[k];
+    if (t >= total) break;
+    if (threadIdx.x == 0) s_task[k ^ 1] = atomicAdd(ticket, 1u);
+    // pipelined order: block b = [stage 0 of window b, stage 1 of window b-1,
+    // stage 2 of window b-2]; a task's producer is ~3 windows of tiles earlier
+    int s = 0, w = 0;
+    unsigned q = t;
+    for (int b = 0;; ++b) {
+      const int s_lo = b - (nw - 1) > 0 ? b - (nw - 1) : 0, s_hi = b < ns - 1 ? b : ns - 1;
+      const unsigned size = (unsigned)(s_hi - s_lo + 1) * per_stage;
+      if (q < size) { s = s_lo + (int)(q / per_stage); w = b - s; q %= per_stage; break; }
+      q -= size;
+    }
+    const int p = w * W + (int)(q / TPP), j = (int)(q % TPP);
+    if (s > 0) {
+      if (threadIdx.x == 0) {
+        const unsigned* c = done + 3 * p + (s - 1);
+        int it = 0;
+        while (ld_acquire_u32(c) < (unsigned)TPP) {
+          // after one timeout every later wait gives up at once
+          if (++it > PLANE_WAIT_LIMIT || (*(volatile int*)sw.status & ST_TIMEOUT)) {
+            atomicOr(sw.status, ST_TIMEOUT);
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __syncthreads();
+    }
+    const int tile = p * TPP + j;
+    const FastOps op = s == 0 ? job.op[0] : (s == 1 ? job.op[1] : job.op[2]);
+    if (s == job.zstage) fast_body<N, FZ, R, MZ, true>(ph, sw, op, tile, N * TPP);
+    else fast_body<N, FY, R, FM_PLAIN, true>(ph, sw, op, tile, N * TPP);
+    // release the tile: the barrier orders every thread's stores before thread
+    // 0's gpu-scope fence, which makes them visible before the count
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(done + 3 * p + s, 1u);
+    }
+  }
+  // the last block to finish resets the counters for the next launch (every
+  // other block has taken its final ticket by then)
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(finished, 1u) == gridDim.x - 1) {
+      for (int i = 0; i < 3 * N; ++i) done[i] = 0u;
+      *ticket = 0u;
+      __threadfence();
+      *finished = 0u;
+    }
+  }
+}
+
+template <int N, typename R, int MZ>
+__global__ void __launch_bounds__(FastCfg<N, R>::T, 768 / FastCfg<N, R>::T) k_plane(Phys ph, Sweep sw,
+                                                                                    PlaneJob job) {
+  plane_body<N, R, MZ>(ph, sw, job);
 }
 
 }  // namespace gpe

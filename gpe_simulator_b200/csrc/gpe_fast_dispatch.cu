@@ -10,6 +10,9 @@ template <int N, typename R>
 cudaError_t launch_fastb_n(int ax, const Phys* phs, const Sweep* sws, int count, const FastOps& op,
                            cudaStream_t st);
 
+template <int N, typename R>
+cudaError_t launch_plane_n(int mz, const Phys& ph, const Sweep& sw, PlaneJob job, cudaStream_t st);
+
 #define GPE_FAST_SIZES(X) X(32) X(48) X(64) X(96) X(128) X(160) X(256)
 
 template <typename R>
@@ -33,6 +36,18 @@ cudaError_t launch_fast_batch(int n, int ax, const Phys* phs, const Sweep* sws, 
   }
 }
 
+// plane-fused y/z sweeps: complex64, n = 128 and 256
+template <typename R>
+cudaError_t launch_plane(int n, int mz, const Phys& ph, const Sweep& sw, const PlaneJob& job, cudaStream_t st) {
+  if (sizeof(R) != 4) return cudaErrorInvalidValue;
+  switch (n) {
+    case 128: return launch_plane_n<128, float>(mz, ph, sw, job, st);
+    case 256: return launch_plane_n<256, float>(mz, ph, sw, job, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template cudaError_t launch_plane<float>(int, int, const Phys&, const Sweep&, const PlaneJob&, cudaStream_t);
 template cudaError_t launch_fast<float>(int, int, const Phys&, const Sweep&, const FastOps&, cudaStream_t);
 template cudaError_t launch_fast<double>(int, int, const Phys&, const Sweep&, const FastOps&, cudaStream_t);
 template cudaError_t launch_fast_batch<float>(int, int, const Phys*, const Sweep*, int, const FastOps&,

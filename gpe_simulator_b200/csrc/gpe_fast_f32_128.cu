@@ -4,3 +4,5 @@ template cudaError_t gpe::launch_fast_n<128, float>(int, const gpe::Phys&, const
                                                  const gpe::FastOps&, cudaStream_t);
 template cudaError_t gpe::launch_fastb_n<128, float>(int, const gpe::Phys*, const gpe::Sweep*, int,
                                                   const gpe::FastOps&, cudaStream_t);
+template cudaError_t gpe::launch_plane_n<128, float>(int, const gpe::Phys&, const gpe::Sweep&, gpe::PlaneJob,
+                                                     cudaStream_t);

@@ -85,4 +85,52 @@ cudaError_t launch_fastb_n(int ax, const Phys* phs, const Sweep* sws, int count,
   return launch_fastb_one<N, FX, R, FM_PLAIN>(phs, sws, count, op, st);
 }
 
+// Persistent plane-fused launch: one block per resident slot.  The scheduling
+// window is the smallest divisor W of N for which a producer task is handed out
+// at least AHEAD x (tickets in flight = 2 per block) tickets before its
+// consumers; the producer-consumer distance is stages x W x N/L tickets.
+template <int N, typename R, int MZ>
+static cudaError_t launch_plane_one(const Phys& ph, const Sweep& sw, PlaneJob job, cudaStream_t st) {
+  constexpr int L = FastCfg<N, R>::L;
+  constexpr int T = FastCfg<N, R>::T;
+  constexpr int TPP = N / L;
+  constexpr size_t smem = fast_smem_bytes<N, R>();
+  static int attr_dev = -1, resident = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaError_t e = cudaFuncSetAttribute(k_plane<N, R, MZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_plane<N, R, MZ>, T, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    resident = (per_sm > 0 ? per_sm : 1) * sms;
+    attr_dev = dev;
+  }
+  if (job.nstage < 1 || job.nstage > 3 || job.zstage < 0 || job.zstage >= job.nstage) return cudaErrorInvalidValue;
+#ifndef GPE_PLANE_AHEAD
+#define GPE_PLANE_AHEAD 1
+#endif
+  int w = N;
+  for (int c = 1; c <= N; ++c)
+    if (N % c == 0 && c * TPP * job.nstage >= GPE_PLANE_AHEAD * 2 * resident) { w = c; break; }
+  job.window = w;
+  const int tasks = N * TPP * job.nstage;
+  const int grid = resident < tasks ? resident : tasks;
+  k_plane<N, R, MZ><<<grid, T, smem, st>>>(ph, sw, job);
+  return cudaGetLastError();
+}
+
+template <int N, typename R>
+cudaError_t launch_plane_n(int mz, const Phys& ph, const Sweep& sw, PlaneJob job, cudaStream_t st) {
+  switch (mz) {
+    case FM_Z1: return launch_plane_one<N, R, FM_Z1>(ph, sw, job, st);
+    case FM_Z2: return launch_plane_one<N, R, FM_Z2>(ph, sw, job, st);
+    case FM_Z21: return launch_plane_one<N, R, FM_Z21>(ph, sw, job, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 }  // namespace gpe

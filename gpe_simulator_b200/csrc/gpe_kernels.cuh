@@ -381,19 +381,21 @@ __device__ void setup_ctx(const Phys& ph, const Sweep& sw, unsigned all_ops, PwC
 
 // Finish a norm reduction: the last block to arrive sums all partials in a
 // fixed order and stores sqrt(N) and 1/sqrt(N).
-static __device__ void norm_finish(const Phys& ph, const Sweep& sw, Acc total, Acc* sh) {
+// Partial `total` of tile `idx` of `count`; the block that finishes last sums the
+// partials in index order (deterministic) and publishes the renormalisation scale.
+static __device__ void norm_finish_n(const Phys& ph, const Sweep& sw, Acc total, Acc* sh, int idx, int count) {
   __shared__ bool last;
   if (threadIdx.x == 0) {
-    sw.partial[blockIdx.x] = total.value();
+    sw.partial[idx] = total.value();
     __threadfence();
     const unsigned t = atomicAdd(sw.ticket, 1u);
-    last = (t == gridDim.x - 1);
+    last = (t == (unsigned)count - 1);
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
   Acc a[1];
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) a[0].add(__ldcg(sw.partial + b));
+  for (int b = threadIdx.x; b < count; b += blockDim.x) a[0].add(__ldcg(sw.partial + b));
   block_merge<1>(a, sh);
   if (threadIdx.x == 0) {
     const double N = a[0].value() * ph.dx3;
@@ -404,6 +406,10 @@ static __device__ void norm_finish(const Phys& ph, const Sweep& sw, Acc total, A
     sw.scale[2] = N;
     *sw.ticket = 0u;
   }
+}
+
+static __device__ void norm_finish(const Phys& ph, const Sweep& sw, Acc total, Acc* sh) {
+  norm_finish_n(ph, sw, total, sh, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- the sweep kernel

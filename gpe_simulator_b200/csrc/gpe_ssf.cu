@@ -9,6 +9,8 @@ cudaError_t launch_fast(int n, int ax, const Phys& ph, const Sweep& sw, const Fa
 template <typename R>
 cudaError_t launch_fast_batch(int n, int ax, const Phys* phs, const Sweep* sws, int count, const FastOps& op,
                               cudaStream_t st);
+template <typename R>
+cudaError_t launch_plane(int n, int mz, const Phys& ph, const Sweep& sw, const PlaneJob& job, cudaStream_t st);
 }
 
 #include <algorithm>
@@ -218,6 +220,7 @@ struct gpe_plan {
   int lt_z = 1, lt_yx = 16;
   bool gen = false;                // grid size needs the odd-prime radices 7/11/13
   bool fast = false;               // register-resident sweeps exist for this n
+  bool plane = false;              // y and z sweeps fused per x-plane (opt-in; complex64, n = 128, 256)
   int ept = 16;                    // elements per thread of the sweep family
   int nbins = 0;
   double shell_w = 0;
@@ -235,6 +238,7 @@ struct gpe_plan {
   void* d_tw = nullptr;
   double* d_partial = nullptr;   // 2 areas of 4*max_tiles doubles
   unsigned* d_ticket = nullptr;
+  unsigned* d_plane = nullptr;   // plane-fused launches: ticket, finished blocks, per (plane, stage) counts
   double* d_scale = nullptr;     // [sqrtN, 1/sqrtN, N, ...]
   int* d_status = nullptr;
   double* d_hist = nullptr;
@@ -348,6 +352,46 @@ int fsweep(gpe_plan* p, int ax, Sweep sw, const FastOps& op, cudaStream_t st) {
   return GPE_OK;
 }
 
+// One plane-fused launch: up to three consecutive y/z sweeps of psi (in place),
+// stage `zstage` a z sweep of mode `mz`, the others y sweeps.  Recorded as a z
+// launch in the per-axis profile.
+int psweep(gpe_plan* p, void* psi, int mz, const FastOps* ops, int nstage, int zstage, double t1, double t2,
+           cudaStream_t st) {
+  Sweep sw;
+  memset(&sw, 0, sizeof(sw));
+  sw.src = psi;
+  sw.dst = psi;
+  sw.t1 = t1;
+  sw.t2 = t2;
+  sw.partial = p->d_partial;
+  sw.pp = p->pp;
+  sw.tw = p->d_tw;
+  sw.tw_lo = (const char*)p->d_tw + (size_t)p->n * p->csize;
+  sw.ticket = p->d_ticket;
+  sw.scale = p->d_scale;
+  sw.status = p->d_status;
+  PlaneJob job;
+  memset(&job, 0, sizeof(job));
+  for (int i = 0; i < nstage; ++i) job.op[i] = ops[i];
+  job.nstage = nstage;
+  job.zstage = zstage;
+  job.ctr = p->d_plane;
+  gpe_plan::Rec r{AX_Z, nullptr, nullptr};
+  if (p->prof) {
+    r.a = pooled_event(p);
+    r.b = pooled_event(p);
+    CU(cudaEventRecord(r.a, st));
+  }
+  const cudaError_t e = launch_plane<float>(p->n, mz, p->ph, sw, job, st);
+  if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("plane sweep: ") + cudaGetErrorString(e));
+  ++p->launches;
+  if (p->prof) {
+    CU(cudaEventRecord(r.b, st));
+    p->recs.push_back(r);
+  }
+  return GPE_OK;
+}
+
 FastOps mk_ops(int mode, int inv1 = 0, int invm = 0, int scale = 0, int norm = 0) {
   FastOps o;
   o.mode = mode; o.inv1 = inv1; o.invm = invm; o.scale = scale; o.norm = norm;
@@ -428,8 +472,9 @@ int fill_plan(gpe_plan* p, const gpe_desc* d) {
     if (p->pp.radix[q] > 5 && p->pp.radix[q] != 8 && p->pp.radix[q] != 16) p->gen = true;
   p->ept = p->gen ? 8 : 16;
   // register-resident sweeps: n = 32, 48, 64, 96, 128, 160, 256; potentials from tables (no per-point program)
-  p->fast = (n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 160 || n == 256) && !d->generic_only &&
-            d->dynamic_g_len == 0;
+  p->fast = (n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 160 || n == 256) &&
+            d->generic_only != 1 && d->dynamic_g_len == 0;
+  p->plane = p->fast && d->dtype == GPE_C64 && (n == 128 || n == 256) && d->generic_only == 3;
   const int emax = 512 * p->ept;
   p->lt_yx = std::max(1, std::min(d->dtype == GPE_C64 ? 16 : 8, emax / n));
   p->lt_z = std::max(1, std::min(n * n, std::min(4096, emax) / n));
@@ -517,7 +562,7 @@ void free_plan(gpe_plan* p) {
   for (auto e : p->pool) cudaEventDestroy(e);
   void* bufs[] = {p->d_x, p->d_k, p->d_kin, p->d_kth, p->d_vax, p->d_vre, p->d_vim, p->d_prog_g, p->d_dyn,
                   p->d_tw, p->d_partial, p->d_ticket, p->d_scale, p->d_status, p->d_hist, p->d_out,
-                  p->d_work};
+                  p->d_work, p->d_plane};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete p;
@@ -559,6 +604,10 @@ int create(const gpe_desc* d, gpe_plan** out) {
   CU(cudaMalloc(&p->d_partial, 2 * 4 * (size_t)p->max_tiles * sizeof(double)));
   CU(cudaMalloc(&p->d_ticket, sizeof(unsigned)));
   CU(cudaMemset(p->d_ticket, 0, sizeof(unsigned)));
+  if (p->plane) {
+    CU(cudaMalloc(&p->d_plane, (2 + 3 * (size_t)n) * sizeof(unsigned)));
+    CU(cudaMemset(p->d_plane, 0, (2 + 3 * (size_t)n) * sizeof(unsigned)));
+  }
   CU(cudaMalloc(&p->d_scale, 4 * sizeof(double)));
   const double one[4] = {1.0, 1.0, 1.0, 0.0};
   CU(cudaMemcpy(p->d_scale, one, sizeof(one), cudaMemcpyHostToDevice));
@@ -795,6 +844,34 @@ int gpe_step(gpe_plan* p, void* psi, int nsteps, long long step0, void* stream) 
   if (nsteps < 0) return fail(GPE_ERR_ARG, "nsteps must be >= 0");
   cudaStream_t st = (cudaStream_t)stream;
   const bool imag = p->kind == GPE_IMAGINARY;
+  if (p->plane && nsteps > 0) {
+    // per step: XKIN, then one plane-fused launch [inverse y, z, forward y]; the
+    // first call opens with [Z1, forward y], the last step ends with [inverse y, Z2]
+    const FastOps yf = mk_ops(FM_PLAIN), yi = mk_ops(FM_PLAIN, 1);
+    {
+      const FastOps ops[2] = {mk_ops(FM_Z1), yf};
+      TRY(psweep(p, psi, FM_Z1, ops, 2, 0, t_mid_host(p, step0), 0.0, st));
+    }
+    for (int s = 0; s < nsteps; ++s) {
+      const double t = t_mid_host(p, step0 + s), tn = t_mid_host(p, step0 + s + 1);
+      Sweep x = mk_sweep(psi, psi);
+      TRY(fsweep(p, AX_X, x, mk_ops(FM_XKIN), st));
+      const bool more = s + 1 < nsteps;
+      if (more && !imag) {
+        const FastOps ops[3] = {yi, mk_ops(FM_Z21), yf};
+        TRY(psweep(p, psi, FM_Z21, ops, 3, 1, t, tn, st));
+        continue;
+      }
+      const FastOps ops[2] = {yi, mk_ops(FM_Z2, 0, 0, 0, imag ? 1 : 0)};
+      TRY(psweep(p, psi, FM_Z2, ops, 2, 1, t, 0.0, st));
+      if (more) {
+        const FastOps ops2[2] = {mk_ops(FM_Z1, 0, 0, 1), yf};
+        TRY(psweep(p, psi, FM_Z1, ops2, 2, 0, tn, 0.0, st));
+      }
+    }
+    if (imag) TRY(scale_sweep(p, psi, st));
+    return GPE_OK;
+  }
   if (p->fast && nsteps > 0) {
     // real time fuses each step's last z sweep with the next step's first
     TRY(fast_front(p, psi, t_mid_host(p, step0), false, st));

@@ -117,8 +117,12 @@ typedef struct gpe_desc {
     /* complex64 plans: 1 = evaluate and apply the local half-step factor in FP64
      * (0 = FP32 phase evaluation); ignored for complex128 */
     int local_fp64;
-    /* 1 = use the generic mixed-radix sweeps even where register-resident sweeps
-     * exist (n = 64, 128, 256); for testing one path against the other */
+    /* sweep path: 0 = fastest available (register-resident sweeps for n = 32, 48,
+     * 64, 96, 128, 160, 256, else generic); 1 = generic mixed-radix sweeps only;
+     * 2 = same as 0; 3 = complex64 n = 128, 256: the y and z sweeps of each
+     * x-plane fused into one persistent launch (psi crosses HBM once per launch
+     * instead of once per sweep; identical results, measured slower on B200
+     * because the sweeps are issue-bound, not HBM-bound). */
     int generic_only;
 } gpe_desc;
 
