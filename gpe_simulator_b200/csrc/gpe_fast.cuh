@@ -125,11 +125,11 @@ __device__ __forceinline__ void slot(int gs, int per, int& l, int& lane) {
 // slots).  Out: v[s][a] = X[lane_s + B*a] (phase-2 slots with B lanes per line).
 template <int N, int A, int B, int AX, typename R, int QA, int QB, int V>
 __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename Cx<R>::T* ex,
-                                           const typename Cx<R>::T* tw, const typename Cx<R>::T* twl) {
+                                           const typename TwE<R>::T* tw) {
   // In: QA slots of (A lanes, B values), slot s holding x[lane + A*b] in v[s*B + b].
   // Out: QB slots of (B lanes, A values), slot s holding X[lane + B*a] in v[s*A + a].
-  // tw/twl: 2-D twiddle table of this split, tw[k2*A + lane] = W_N^(lane*k2) (hi, lo):
-  // consecutive lanes read consecutive entries (no bank conflicts in Z tiles).
+  // tw: 2-D twiddle table of this split, tw[k2*A + lane] = W_N^(lane*k2) ({hi, lo}
+  // for complex64): consecutive lanes read consecutive entries.
   using C = typename Cx<R>::T;
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
@@ -145,12 +145,9 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
     int l, lane;
     slot<AX, L>(gs, A, l, lane);
     C* x = v + s * B;
-    Dft<B>::run(x, tw, twl, N / B);
+    Dft<B>::run(x, (const C*)nullptr, (const C*)nullptr, N / B);
 #pragma unroll
-    for (int k2 = 1; k2 < B; ++k2) {
-      const int e = k2 * A + lane;
-      x[k2] = twmul(x[k2], tw[e], twl[e]);
-    }
+    for (int k2 = 1; k2 < B; ++k2) x[k2] = tw_apply(x[k2], tw[k2 * A + lane]);
     // exchange layout: Z tiles [l][k2][A + 1] (odd pitch), P tiles [k2][lane][L]
 #pragma unroll
     for (int k2 = 0; k2 < B; ++k2) {
@@ -172,7 +169,7 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
       const int idx = AX == FZ ? (l * B + k2) * (A + 1) + n1 : (k2 * A + n1) * L + l;
       x[n1] = ex[idx];
     }
-    Dft<A>::run(x, tw, twl, N / A);
+    Dft<A>::run(x, (const C*)nullptr, (const C*)nullptr, N / A);
   }
   if (WARP_LOCAL) __syncwarp(); else __syncthreads();
 }
@@ -207,6 +204,18 @@ __device__ __forceinline__ void sin_cosm1_series(float x, float& s, float& cm1) 
                                            2.4801587301587302e-05f), -1.3888888888888889e-03f),
                            4.1666666666666667e-02f), -0.5f);
   }
+}
+
+// Short forms for |x| <= 1/8 (first omitted terms x^7/7!, x^8/8!: below 8e-10
+// of the result), the common case of real-time steps.
+__device__ __forceinline__ void sin_cosm1_tiny(float x, float& s, float& cm1) {
+  const float z = x * x;
+  s = x * fmaf(z, fmaf(z, 8.3333333333333333e-03f, -1.6666666666666667e-01f), 1.0f);
+  cm1 = z * fmaf(z, fmaf(z, -1.3888888888888889e-03f, 4.1666666666666667e-02f), -0.5f);
+}
+__device__ __forceinline__ float expm1_tiny(float x) {
+  return x * fmaf(x, fmaf(x, fmaf(x, fmaf(x, fmaf(x, 1.3888888888888889e-03f, 8.3333333333333333e-03f),
+         4.1666666666666667e-02f), 1.6666666666666667e-01f), 0.5f), 1.0f);
 }
 
 // exp(x) - 1 from its Taylor series, valid for |x| <= 1/2 (first omitted term
@@ -319,8 +328,10 @@ __device__ __forceinline__ void kin_all(typename Cx<R>::T (&v)[EPT], const Phys&
 
 // One local half-step over all registers (layout LANES x VALS, element m = lane +
 // LANES*a, Z tiles: m = z index), potential vz[m] + ctab[l] (+ arrays).  The
-// phases are computed first; whether all of this thread's phases lie in the
-// series' range is decided once, so each element loop is straight-line code.
+// phases are computed first; which series covers all phases of the warp
+// (|phase| <= 1/8: short series; <= pi/4 (1/2 in imaginary time): full
+// series; else library sincosf/expm1f) is decided once per warp, so each
+// element loop is straight-line code without divergence.
 // TWO: two consecutive real-time half-steps at one point as one rotation by
 // (2 vz[m] + ctab[l] + 2 beta |psi|^2) dt/2 with ctab = c1 + c2; exact because
 // the first rotation leaves |psi| unchanged (callers pass beta already doubled).
@@ -333,7 +344,7 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
   constexpr int E = SLOTS * VALS;
   R phs[E];
   R gam[ARR ? E : 1];
-  bool small = true;
+  bool small = true, tiny = true;
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) {
     if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
@@ -352,8 +363,11 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
       const typename Cx<R>::T x = v[e];
       phs[e] = (V + beta * (x.x * x.x + x.y * x.y)) * h;
       small = small && fabs(phs[e]) <= (REAL ? (R)0.78539816 : (R)0.5);
+      tiny = tiny && fabs(phs[e]) <= (R)0.125;
     }
   }
+  small = __all_sync(0xffffffffu, small);
+  tiny = __all_sync(0xffffffffu, tiny);
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) {
     if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
@@ -371,6 +385,16 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
           sincos((double)phs[e], &sd, &cd);
           if (ARR) { const double am = exp((double)gam[e]); sd *= am; cd *= am; }
           v[e] = mk((R)(x.x * cd + x.y * sd), (R)(x.y * cd - x.x * sd));
+        }
+      } else if (tiny) {
+        if (!REAL) {
+          const float em = expm1_tiny((float)-phs[e]);
+          v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
+        } else {
+          float sn, cm1;
+          sin_cosm1_tiny((float)phs[e], sn, cm1);
+          if (ARR) { const float am = expm1f((float)gam[e]); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
+          v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
         }
       } else if (small) {
         if (!REAL) {
@@ -514,10 +538,9 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   constexpr int S1 = FastCfg<N, R>::Q1;   // slots in layout (N1 lanes, N2 values)
   constexpr int S2 = FastCfg<N, R>::Q2;   // slots in layout (N2 lanes, N1 values)
   constexpr bool ZM = MODE == FM_Z1 || MODE == FM_Z2 || MODE == FM_Z21;
+  using TW = typename TwE<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tw = (C*)smem_raw;
-  C* twl = tw + N;
-  C* ex = twl + N;
+  C* ex = (C*)smem_raw + 2 * N;   // after the twiddle table (N entries of 16 bytes)
   Acc* red = (Acc*)(ex + fast_exchange_elems<N, R>());
   unsigned char* tail = (unsigned char*)(red + 32 * 4);
   FastTables<R> tb;
@@ -529,22 +552,23 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   tb.c1 = tb.vz + N;
   tb.c2 = tb.c1 + L;
   tb.c12 = tb.c2 + L;
-  // 2-D twiddle tables: t1 for the split (N1 lanes, N2 values), t2 for (N2, N1)
-  C* t1 = tw;
-  C* t1l = twl;
-  C* t2 = (N1 == N2) ? t1 : (C*)(tail + fast_tables_bytes<N, R>());
-  C* t2l = (N1 == N2) ? t1l : t2 + N;
+  // 2-D twiddle tables: t1 for the split (N1 lanes, N2 values), t2 for (N2, N1);
+  // complex64 entries pack hi and lo
+  TW* t1 = (TW*)smem_raw;
+  TW* t2 = (N1 == N2) ? t1 : (TW*)(tail + fast_tables_bytes<N, R>());
   {
-    const C* g = (const C*)sw.tw;
+    const C* gh = (const C*)sw.tw;
     const C* gl = (const C*)sw.tw_lo;
+    auto entry = [&](int e) -> TW {
+      if constexpr (sizeof(R) == 4) return make_float4(gh[e].x, gh[e].y, gl[e].x, gl[e].y);
+      else return gh[e];
+    };
     for (int q = threadIdx.x; q < N; q += T) {
-      const int k2 = q / N1, n1 = q % N1;   // t1[k2*N1 + n1] = W^(n1*k2)
-      t1[q] = g[n1 * k2];                 // n1*k2 < N
-      t1l[q] = gl[n1 * k2];
+      const int k2 = q / N1, n1 = q % N1;   // t1[k2*N1 + n1] = W^(n1*k2), n1*k2 < N
+      t1[q] = entry(n1 * k2);
       if (N1 != N2) {
         const int k2b = q / N2, n2 = q % N2;  // t2[k1*N2 + n2] = W^(n2*k1)
-        t2[q] = g[n2 * k2b];
-        t2l[q] = gl[n2 * k2b];
+        t2[q] = entry(n2 * k2b);
       }
     }
   }
@@ -563,12 +587,12 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   fast_load<N, AX, R, S1, CG>(v, tl, (const C*)sw.src, MODE == FM_Z2 || MODE == FM_Z21 || (MODE == FM_PLAIN && op.inv1));
   __syncthreads();  // twiddles and tables visible
   if (MODE == FM_Z1) fast_pointwise<N, AX, R, MODE, 0, N1, N2, S1>(v, tl, ph, tb, op, cx);
-  fft_2phase<N, N1, N2, AX, R, S1, S2, EPT>(v, ex, t1, t1l);
+  fft_2phase<N, N1, N2, AX, R, S1, S2, EPT>(v, ex, t1);
   if (MODE == FM_Z21 || MODE == FM_XKIN) {
     if (MODE == FM_Z21) conj_all(v);  // finish the inverse before the physics
     fast_pointwise<N, AX, R, MODE, 1, N2, N1, S2>(v, tl, ph, tb, op, cx);
     if (MODE == FM_XKIN) conj_all(v);  // start the inverse
-    fft_2phase<N, N2, N1, AX, R, S2, S1, EPT>(v, ex, t2, t2l);
+    fft_2phase<N, N2, N1, AX, R, S2, S1, EPT>(v, ex, t2);
     if (MODE == FM_XKIN) conj_all(v);
     fast_store<N, AX, R, N1, N2, S1>(v, tl, (C*)sw.dst);
   } else {

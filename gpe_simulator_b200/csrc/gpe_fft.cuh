@@ -89,6 +89,17 @@ __device__ __forceinline__ float2 twmul(float2 v, float2 w, float2 l) {
 }
 __device__ __forceinline__ double2 twmul(double2 v, double2 w, double2) { return cmul(v, w); }
 
+// twiddle-table entries of the register-resident sweeps: complex64 keeps the
+// {hi, lo} pair of a twiddle in one 16-byte entry (one shared-memory load),
+// complex128 the twiddle itself
+template <typename R> struct TwE;
+template <> struct TwE<float>  { using T = float4; };
+template <> struct TwE<double> { using T = double2; };
+__device__ __forceinline__ float2 tw_apply(float2 v, float4 w) {
+  return twmul(v, make_float2(w.x, w.y), make_float2(w.z, w.w));
+}
+__device__ __forceinline__ double2 tw_apply(double2 v, double2 w) { return cmul(v, w); }
+
 // v * W_16^q, W_16 = exp(-2 pi i / 16), q known at compile time after unrolling
 template <typename C> __device__ __forceinline__ C mul_w16(C v, int q) {
   using R = decltype(v.x);
