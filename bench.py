@@ -10,6 +10,12 @@ Gaussian beam A = 10, w = 0.5, R = 2, angular rate ramped 0 -> 0.5 over the firs
 an exact reparametrisation.  Inputs are synthetic (seeded noisy Gaussian relaxed
 for 50 imaginary-time steps); psi is 128 MiB, larger than the 126 MB L2.
 
+On one GPU the line also carries ``batched`` (64 imaginary-time solves of mixed
+grid sizes as one running batch vs one at a time: solves/s) and ``serving`` (a
+seeded request stream through the continuous-batching server vs the plain path:
+solves/s, p50/p99 latency, results identical) -- the other two parts of the
+metric.
+
 ``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]``
 prints one JSON line (rank 0).  Multi-GPU runs are independent replicas (one
 solve per GPU, weak scaling); ``value`` is the whole-job steps/s.
@@ -274,7 +280,79 @@ def ours(args, world, rank, local):
     }
     if world == 1 and rank == 0 and not args.no_cpu:
         result["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+    if world == 1 and not args.no_batch:
+        result["batched"] = batched_leg()
+    if world == 1 and not args.no_serve:
+        result["serving"] = serving_leg(args.serve_requests, args.serve_rate)
     return result, plan
+
+
+def batched_leg():
+    """Batched parameter sweep: 64 imaginary-time solves (grids 48^3..160^3, g
+    log-uniform in [100, 5000], trap aspect ratios in [0.5, 2], complex64, dt =
+    1e-3 in oscillator units) run to |dE|/E < 1e-9 per step or 5000 steps, as one
+    running batch and one at a time through single plans with the same
+    convergence checks (every 10 steps).  Wall-clock seconds, states resident."""
+    import torch
+    from gpe_simulator_b200.batch import Batch, initial_states, solve_alone, sweep_instances
+    insts = sweep_instances(64, seed=1)
+    states = initial_states(insts, torch.complex64)
+    batch = Batch(insts, torch.complex64)
+    work = [st.clone() for st in states]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    steps, final = batch.solve(work, tol=1e-9, max_steps=5000, check_every=10)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    launches = batch.launch_count()
+    batch.close()
+    t0 = time.perf_counter()
+    alone = []
+    for inst, st in zip(insts, states):
+        alone.append(solve_alone(inst, st.clone(), torch.complex64, tol=1e-9, max_steps=5000, check_every=10))
+    torch.cuda.synchronize()
+    t_alone = time.perf_counter() - t0
+    a_steps = np.array([a[0] for a in alone])
+    a_diag = np.array([a[1] for a in alone])
+    e_diff = float(np.max(np.abs(final[:, 4] - a_diag[:, 4]) / np.abs(a_diag[:, 4])))
+    return {"instances": len(insts), "grids": sorted({i.n for i in insts}),
+            "solves_per_s": len(insts) / t_batch, "wall_s": t_batch,
+            "one_at_a_time_solves_per_s": len(insts) / t_alone, "one_at_a_time_wall_s": t_alone,
+            "speedup": t_alone / t_batch, "steps_median": int(np.median(steps)), "steps_max": int(steps.max()),
+            "same_steps_as_alone": bool(np.array_equal(steps, a_steps)),
+            "E_max_rel_diff_vs_alone": e_diff, "gpu_launches": int(launches),
+            "criterion": "|E_k - E_{k-10}| / (10 |E_k|) < 1e-9 or 5000 steps"}
+
+
+def serving_leg(count, rate):
+    """Serving stream (bounded sample of the 1000-request stream): seeded Poisson
+    arrivals at `rate`/s, 70% imaginary-time ground states 32^3..128^3 and 30%
+    real-time stirring segments of 500-5000 steps on 8 resident states 64^3..256^3,
+    complex64, 150 GB budget; the continuous-batching server against the plain
+    one-at-a-time path on the same stream.  Results must be identical."""
+    import torch
+    from gpe_simulator_b200 import serve
+    reqs = serve.workload(count, rate=rate, seed=2)
+    sess = serve.make_sessions()
+    t0 = time.perf_counter()
+    serve.Server(sess, budget=150e9).run(reqs)
+    wall = time.perf_counter() - t0
+    mixed = serve.summarise(reqs)
+    reqs2 = serve.workload(count, rate=rate, seed=2)
+    sess2 = serve.make_sessions()
+    serve.run_plain(reqs2, sess2)
+    plain = serve.summarise(reqs2)
+    same = all(a.taken == b.taken and (a.kind != "imaginary" or torch.equal(a.result["psi"], b.result["psi"]))
+               for a, b in zip(reqs, reqs2))
+    same = same and all(torch.equal(x.psi, y.psi) for x, y in zip(sess, sess2))
+    out = {"requests": count, "rate_per_s": rate, "imaginary": sum(r.kind == "imaginary" for r in reqs),
+           "solves_per_s": mixed["solves_per_s"], "p50_ms": mixed["p50_ms"], "p99_ms": mixed["p99_ms"],
+           "plain_solves_per_s": plain["solves_per_s"], "plain_p50_ms": plain["p50_ms"],
+           "plain_p99_ms": plain["p99_ms"], "speedup": mixed["solves_per_s"] / plain["solves_per_s"],
+           "results_identical_to_plain": bool(same), "wall_s": wall}
+    for s_ in sess + sess2:
+        s_.plan.close()
+    return out
 
 
 def cpu_baseline(budget_s, steps_cap=None):
@@ -326,6 +404,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=40)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-requests", type=int, default=60)
+    ap.add_argument("--serve-rate", type=float, default=50.0)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -175,6 +175,31 @@ class Batch:
         return steps, final
 
 
+def solve_alone(inst, psi, dtype=torch.complex64, tol=1e-9, max_steps=5000, check_every=10):
+    """One instance through a single plan with the convergence rule of
+    :meth:`Batch.solve` (same checks, same step counts): the one-at-a-time
+    baseline of a batched solve.  Returns ``(steps, diagnostics)``."""
+    from .plan import Plan
+    plan = Plan(inst.n, inst.x, inst.k, dtype=dtype, kind="imaginary", beta=inst.beta, dt=inst.dt,
+                kinetic_coeff=inst.kinetic_coeff, static_expr=inst.static_expr)
+    try:
+        keys = ("N", "E_kin", "E_pot", "E_int", "E", "mu")
+        d = plan.diagnostics(psi)
+        last, steps = d["E"], 0
+        while steps < max_steps:
+            chunk = int(min(check_every, max_steps - steps))
+            plan.step(psi, chunk)
+            steps += chunk
+            d = plan.diagnostics(psi)
+            rate = abs(d["E"] - last) / (chunk * abs(d["E"])) if d["E"] != 0 else float("inf")
+            last = d["E"]
+            if rate < tol:
+                break
+        return steps, np.array([d[k] for k in keys])
+    finally:
+        plan.close()
+
+
 def sweep_instances(count=64, seed=1, dt=1e-3):
     """The batched parameter sweep, in reference units.
 
