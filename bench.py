@@ -83,6 +83,13 @@ def max_over_ranks(value, world, device=None):
     return float(t.item())
 
 
+def job_throughput(ms, steps, world, device=None):
+    """Whole-job steps/s of `world` replicas that each ran `steps` steps: the
+    slowest rank's device time sets the job time.  Returns (max ms, steps/s)."""
+    ms_max = max_over_ranks(ms, world, device)
+    return ms_max, world * steps / (ms_max / 1e3)
+
+
 def barrier(world, device=None):
     if world > 1:
         import torch.distributed as dist
@@ -202,8 +209,7 @@ def ours(args, world, rank, local):
     launches = launch_count(plan) - n0
     ms = start.elapsed_time(end)
     clocks = sampler.stop()
-    ms_max = max_over_ranks(ms, world, device)
-    value = world * args.steps / (ms_max / 1e3)
+    ms_max, value = job_throughput(ms, args.steps, world, device)
 
     # ---- per-launch durations of the sweeps (events around each launch, same stream)
     profile(plan, True)
@@ -249,8 +255,7 @@ def ours(args, world, rank, local):
         out_host.copy_(st.psi, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, device)
-    e2e = world * e2e_steps / (e2e_ms / 1e3)
+    e2e_ms, e2e = job_throughput(e0.elapsed_time(e1), e2e_steps, world, device)
     nbytes = host.numel() * host.element_size()
 
     result = {

@@ -45,8 +45,8 @@ def launch_stage(stage, on_diagnostics=None):
         want_scalar = any(is_due(i, iv) for iv in scalar)
         want_nk = any(is_due(i, iv) for iv in spectrum)
         if want_scalar or want_nk:
-            plan = prop.binding.plan(stage)
-            rec = plan.diagnostics(stage.psi, t=i * stage.dt, nk=want_nk)
+            plan, psi = prop.binding.plan(stage)
+            rec = plan.diagnostics(psi, t=i * stage.dt, nk=want_nk)
             rec.update(step=i, time=i * stage.dt)
             history.append(rec)
             _write(stage, rec, want_scalar, want_nk)

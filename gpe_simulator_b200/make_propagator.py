@@ -16,12 +16,28 @@ renormalisation scale, kinetic factors and the beam angle).
 
 Each closure also has ``closure.run(stage, nsteps, step0)``: ``nsteps`` steps
 in one C-ABI call with ``t = i*dt`` for step ``i`` (``gpe/launch.py:8-13``).
+
+The stage's arrays may be torch tensors or any CUDA array that exports DLPack
+(the reference's CuPy arrays): they are viewed zero-copy, psi is advanced in
+place, and the closure returns the caller's own ``stage.psi`` object.  Both
+libraries enqueue on the legacy default stream unless told otherwise, so the
+order against the caller's own work is kept.  A ``staticV`` that is not a torch
+tensor is re-read when a different array (or buffer) is bound; the reference
+never modifies it in place.
 """
 
 import torch
 
 from .expressions import from_cuda_text
 from .plan import Plan
+
+
+def _tensor(a):
+    """Torch view of a CUDA array: a torch tensor as is, a DLPack producer (a
+    CuPy array) zero-copy; anything else unchanged (rejected by the checks)."""
+    if isinstance(a, torch.Tensor) or not hasattr(a, "__dlpack__"):
+        return a
+    return torch.utils.dlpack.from_dlpack(a)
 
 
 class _Binding:
@@ -44,8 +60,10 @@ class _Binding:
         self.static_seen = {}
 
     def check(self, stage):
-        """The reference's per-call assertions (``gpe/make_propagator.py:20-36,66-81,117-133``)."""
-        psi, V, k, x, n = stage.psi, stage.staticV, stage.k_array, stage.x_array, stage.N_grids
+        """The reference's per-call assertions (``gpe/make_propagator.py:20-36,66-81,117-133``);
+        returns torch views of (psi, staticV, k_array, x_array)."""
+        psi, V, k, x = (_tensor(a) for a in (stage.psi, stage.staticV, stage.k_array, stage.x_array))
+        n = stage.N_grids
         assert isinstance(psi, torch.Tensor) and psi.is_cuda
         assert isinstance(V, torch.Tensor) and V.is_cuda
         assert psi.dtype in (torch.complex128, torch.complex64)
@@ -60,26 +78,27 @@ class _Binding:
         assert tuple(k.shape) == (n,) and k.is_contiguous()
         assert isinstance(x, torch.Tensor) and x.dtype == torch.float64
         assert tuple(x.shape) == (n,) and x.is_contiguous()
+        return psi, V, k, x
 
     def plan(self, stage):
-        self.check(stage)
-        psi = stage.psi
+        """(plan, torch view of psi) for this call."""
+        psi, V, k, x = self.check(stage)
         key = (psi.dtype, psi.device.index, int(stage.N_grids), float(stage.beta), float(stage.dt),
                id(stage.x_array), id(stage.k_array))
         plan = self.plans.get(key)
         if plan is None:
             with torch.cuda.device(psi.device):
-                plan = Plan(stage.N_grids, stage.x_array, stage.k_array, dtype=psi.dtype,
+                plan = Plan(stage.N_grids, x, k, dtype=psi.dtype,
                             kind=self.kind, beta=stage.beta, dt=stage.dt, kinetic_coeff=self.ckin,
                             static_expr=self.static_expr, dynamic_expr=self.dynamic_expr,
                             k_cut=self.k_cut, beam=self.beam, nk_bins=self.nk_bins)
             self.plans[key] = plan
-        self.sync_static(plan, stage.staticV)
-        return plan
+        self.sync_static(plan, V, stage.staticV)
+        return plan, psi
 
-    def sync_static(self, plan, V):
-        """Re-read ``staticV`` only when it is a new tensor or was modified in place."""
-        stamp = (id(V), V._version, V.data_ptr())
+    def sync_static(self, plan, V, orig):
+        """Re-read ``staticV`` only when it is a new array or (torch) was modified in place."""
+        stamp = (id(orig), getattr(orig, "_version", 0), V.data_ptr())
         if self.static_seen.get(id(plan)) == stamp:
             return
         plan.set_static_potential(None if not bool(torch.any(V != 0)) else V)
@@ -97,17 +116,20 @@ def make_real_propagator(stage):
 
     if not binding.dynamic:
         def time_independent_propagator(stage):
-            binding.plan(stage).step_at(stage.psi, 0.0)
+            plan, psi = binding.plan(stage)
+            plan.step_at(psi, 0.0)
             return stage.psi
         fn = time_independent_propagator
     else:
         def time_dependent_propagator(stage, t):
-            binding.plan(stage).step_at(stage.psi, float(t))
+            plan, psi = binding.plan(stage)
+            plan.step_at(psi, float(t))
             return stage.psi
         fn = time_dependent_propagator
 
     def run(stage, nsteps, step0=0):
-        binding.plan(stage).step(stage.psi, nsteps, step0)
+        plan, psi = binding.plan(stage)
+        plan.step(psi, nsteps, step0)
         return stage.psi
 
     fn.run = run
@@ -121,11 +143,13 @@ def make_imag_propagator(stage):
     binding = _Binding(stage, "imaginary")
 
     def standard_imaginary_step(stage):
-        binding.plan(stage).step(stage.psi, 1, 0)
+        plan, psi = binding.plan(stage)
+        plan.step(psi, 1, 0)
         return stage.psi
 
     def run(stage, nsteps, step0=0):
-        binding.plan(stage).step(stage.psi, nsteps, step0)
+        plan, psi = binding.plan(stage)
+        plan.step(psi, nsteps, step0)
         return stage.psi
 
     standard_imaginary_step.run = run
@@ -143,7 +167,8 @@ def make_real_spatial_kernel(stage):
         old = stage.psi
         stage.psi = psi
         try:
-            binding.plan(stage).halfstep(psi, t)
+            plan, view = binding.plan(stage)
+            plan.halfstep(view, t)
         finally:
             stage.psi = old
         return psi
@@ -158,7 +183,8 @@ def make_imag_spatial_kernel(stage):
         old = stage.psi
         stage.psi = psi
         try:
-            binding.plan(stage).halfstep(psi, t)
+            plan, view = binding.plan(stage)
+            plan.halfstep(view, t)
         finally:
             stage.psi = old
         return psi

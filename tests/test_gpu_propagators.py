@@ -165,3 +165,36 @@ def test_zero_mode_spectrum(cuda):
     assert spec["Nk"][0] == pytest.approx(1)
     np.testing.assert_allclose(spec["Nk"][1:], 0, atol=1e-25)
     assert int(spec["counts"][0]) == 1
+
+
+class DLArray:
+    """A CUDA array that only exports DLPack, as the reference's CuPy arrays do."""
+
+    def __init__(self, t):
+        self.t = t
+
+    def __dlpack__(self, *args, **kwargs):
+        return self.t.__dlpack__(*args, **kwargs)
+
+    def __dlpack_device__(self):
+        return self.t.__dlpack_device__()
+
+
+@pytest.mark.parametrize("kind", ["real", "imaginary"])
+def test_closure_takes_dlpack_arrays_in_place(cuda, kind):
+    """A stage holding foreign (DLPack) arrays is advanced in place, zero-copy,
+    and the closure returns the caller's own psi object."""
+    a = make_stage(kind, n=16, L=8.0, a=50.0, static="x**2+y**2+z**2",
+                   dynamic="0.5*sin(t)*x" if kind == "real" else None)
+    b = make_stage(kind, n=16, L=8.0, a=50.0, static="x**2+y**2+z**2",
+                   dynamic="0.5*sin(t)*x" if kind == "real" else None)
+    raw = b.psi.clone()
+    b.psi, b.staticV = DLArray(raw), DLArray(b.staticV.clone())
+    b.x_array, b.k_array = DLArray(b.x_array.clone()), DLArray(b.k_array.clone())
+    for i in range(3):
+        args = (i * a.dt,) if getattr(a.propagator, "dynamic", False) else ()
+        a.psi = a.propagator(a, *args)
+        out = b.propagator(b, *args)
+        assert out is b.psi
+    torch.cuda.synchronize()
+    assert torch.equal(a.psi, raw)
