@@ -285,11 +285,46 @@ def ours(args, world, rank, local):
     }
     if world == 1 and rank == 0 and not args.no_cpu:
         result["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+    if world == 1 and not args.no_large:
+        result["stir512"] = large_leg()
     if world == 1 and not args.no_batch:
         result["batched"] = batched_leg()
     if world == 1 and not args.no_serve:
         result["serving"] = serving_leg(args.serve_requests, args.serve_rate)
     return result, plan
+
+
+def large_leg(steps=100, warmup=5):
+    """The 512^3 complex64 single solve (same trap, beam, g and dt as the 256^3
+    workload, box [-12,12)^3): steps/s of one multi-step call, state resident."""
+    import torch
+    from gpe_simulator_b200 import Plan, beam_in_reference_units
+    n = 512
+    x = np.linspace(-L_BOX / 2, L_BOX / 2, n, endpoint=False)
+    k = 2 * np.pi * np.fft.fftfreq(n, L_BOX / n)
+    beam = beam_in_reference_units(BEAM["amp"], BEAM["width"], BEAM["radius"], BEAM["omega"],
+                                   BEAM["ramp_steps"] * DT)
+    plan = Plan(n, x, k, dtype=torch.complex64, kind="real", beta=2 * G, dt=DT / 2, static_expr=TRAP_REF,
+                beam=beam)
+    g = torch.from_numpy(np.exp(-x ** 2 / 2)).cuda()
+    psi = (g[:, None, None] * g[None, :, None] * g[None, None, :]).to(torch.complex64).contiguous()
+    plan.normalise(psi)
+    plan.step(psi, warmup, 0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    plan.step(psi, steps, warmup)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    m = n ** 3
+    plan.close()
+    del psi
+    torch.cuda.empty_cache()
+    peak, _ = measured_peak()
+    return {"grid": n, "steps": steps, "steps_per_s": 1e3 / ms, "ms_per_step": ms,
+            "step_roofline_frac": 6 * 8 * m / (ms / 1e3) / 1e9 / peak,
+            "data": "Gaussian trap state, synthetic"}
 
 
 def batched_leg():
@@ -410,6 +445,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep leg")
+    ap.add_argument("--no-large", action="store_true", help="skip the 512^3 leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--serve-requests", type=int, default=60)
     ap.add_argument("--serve-rate", type=float, default=50.0)

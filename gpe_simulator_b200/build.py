@@ -20,7 +20,7 @@ OBJ = PKG / "_build"
 
 FAST_SIZES = (32, 48, 64, 96, 128, 160, 256)
 SOURCES = (["gpe_ssf.cu", "gpe_sweep_f32.cu", "gpe_sweep_f64.cu", "gpe_noalloc.cu", "gpe_fast_dispatch.cu"]
-           + [f"gpe_fast_{p}_{n}.cu" for p in ("f32", "f64") for n in FAST_SIZES])
+           + [f"gpe_fast_{p}_{n}.cu" for p in ("f32", "f64") for n in FAST_SIZES] + ["gpe_fast_f32_512.cu"])
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(INCLUDE),
          "--expt-relaxed-constexpr"]

@@ -21,6 +21,9 @@ cudaError_t launch_fast(int n, int ax, const Phys& ph, const Sweep& sw, const Fa
 #define GPE_CASE(NN) case NN: return launch_fast_n<NN, R>(ax, ph, sw, op, st);
     GPE_FAST_SIZES(GPE_CASE)
 #undef GPE_CASE
+    case 512:
+      if constexpr (sizeof(R) == 4) return launch_fast_n<512, float>(ax, ph, sw, op, st);
+      return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }
 }
@@ -32,6 +35,9 @@ cudaError_t launch_fast_batch(int n, int ax, const Phys* phs, const Sweep* sws, 
 #define GPE_CASE(NN) case NN: return launch_fastb_n<NN, R>(ax, phs, sws, count, op, st);
     GPE_FAST_SIZES(GPE_CASE)
 #undef GPE_CASE
+    case 512:
+      if constexpr (sizeof(R) == 4) return launch_fastb_n<512, float>(ax, phs, sws, count, op, st);
+      return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }
 }
