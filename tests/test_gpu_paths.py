@@ -110,3 +110,23 @@ def test_fast_512_matches_generic(cuda, kind):
     slow.step(b, 4, 0)
     err = (((a - b).abs() ** 2).sum() / (b.abs() ** 2).sum()).sqrt().item()
     assert err < 3e-6, err
+
+
+@pytest.mark.parametrize("kind", ["imaginary", "real"])
+def test_fast_honours_local_fp64(cuda, kind):
+    """local_fp64 (complex64 plans: local factor in FP64) is applied by the
+    register-resident sweeps as by the generic ones."""
+    from gpe_simulator_b200 import Beam
+    kw = dict(beta=800.0, dt=4e-4, static_expr=cases.TRAP, local_fp64=True)
+    if kind == "real":
+        kw["beam"] = Beam(20.0, 0.5, 2.0, 1.0, 0.004)
+    fast, x = make(64, 12.0, kind, torch.complex64, False, **kw)
+    slow, _ = make(64, 12.0, kind, torch.complex64, True, **kw)
+    plain, _ = make(64, 12.0, kind, torch.complex64, False, **{**kw, "local_fp64": False})
+    a = torch.from_numpy(ssf.noisy_gaussian(x, seed=4)).to(torch.complex64).cuda()
+    b, c = a.clone(), a.clone()
+    fast.step(a, 7, 3)
+    slow.step(b, 7, 3)
+    plain.step(c, 7, 3)
+    assert ssf.rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 3e-6
+    assert not torch.equal(a, c)          # the flag changes the arithmetic
