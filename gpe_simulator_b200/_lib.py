@@ -60,6 +60,7 @@ SIGNATURES = {
     "gpe_nk_extraction": [_vp, _vp, _dp, _llp, _vp],
     "gpe_diagnostics": [_vp, _vp, ctypes.c_double, _dp, _dp, _llp, _vp],
     "gpe_status": [_vp, ctypes.POINTER(ctypes.c_int), _vp],
+    "gpe_angular_momentum": [_vp, _vp, _dp, _vp],
     "gpe_launch_count": [_vp, _llp],
     "gpe_profile": [_vp, ctypes.c_int],
     "gpe_profile_read": [_vp, _dp, _llp],

@@ -17,7 +17,8 @@ namespace gpe {
 
 enum : unsigned {
   PW_CONJ_FIRST = 1u, PW_SCALE = 2u, PW_INVM = 4u, PW_HALF1 = 8u, PW_HALF2 = 16u,
-  PW_KIN = 32u, PW_CONJ_LAST = 64u, PW_NORM = 128u, PW_DIAG_R = 256u, PW_DIAG_K = 512u
+  PW_KIN = 32u, PW_CONJ_LAST = 64u, PW_NORM = 128u, PW_DIAG_R = 256u, PW_DIAG_K = 512u,
+  PW_LZ_X = 1024u, PW_LZ_Y = 2048u
 };
 
 enum Axis : int { AX_Z = 0, AX_Y = 1, AX_X = 2 };
@@ -320,6 +321,10 @@ __device__ __forceinline__ typename Cx<R>::T pointwise(const Phys& ph, unsigned 
     sh = min(sh, cx.nbins - 1);
     atomicAdd(cx.hist + sh, w);
   }
+  // angular momentum terms (reference gpe/helper.py:143-156) on data transformed
+  // along z and then x (LZ_X: y k_x |v|^2) or along z and then y (LZ_Y: x k_y |v|^2)
+  if (ops & PW_LZ_X) cx.acc[3].add(ph.x[j] * ph.k[i] * ((double)v.x * v.x + (double)v.y * v.y));
+  if (ops & PW_LZ_Y) cx.acc[3].add(ph.x[i] * ph.k[j] * ((double)v.x * v.x + (double)v.y * v.y));
   return v;
 }
 
@@ -489,7 +494,7 @@ __device__ __forceinline__ void sweep_body(const Phys& ph, const Sweep& sw) {
     block_merge<1>(a, red);
     norm_finish(ph, sw, a[0], red);
   }
-  if (all & (PW_DIAG_R | PW_DIAG_K)) {
+  if (all & (PW_DIAG_R | PW_DIAG_K | PW_LZ_X | PW_LZ_Y)) {
     Acc a[4] = {cx.acc[0], cx.acc[1], cx.acc[2], cx.acc[3]};
     block_merge<4>(a, red);
     if (threadIdx.x == 0)

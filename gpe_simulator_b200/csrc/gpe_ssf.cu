@@ -781,6 +781,47 @@ int diag_launch(gpe_plan* p, const void* psi, double t, cudaStream_t st) {
   return sweep(p, AX_X, s, st);
 }
 
+// Lz of psi (reference gpe/helper.py:143-156).  By Parseval along each axis the
+// reference's slab sums become two k-space sums of the z-transformed state F_z:
+//   Lz = dx^3/n^2 [ sum x k_y |FFT_y F_z|^2 - sum y k_x |FFT_x F_z|^2 ],
+// one forward z sweep into the work buffer and two read-only sweeps (x, y) of it;
+// the per-tile partials are summed on the host in tile order (deterministic).
+int angular_momentum(gpe_plan* p, const void* psi, double* lz, cudaStream_t st) {
+  TRY(ensure_work(p));
+  Sweep s = mk_sweep(psi, p->d_work);
+  s.fft1 = 1;
+  TRY(sweep(p, AX_Z, s, st));
+  s = mk_sweep(p->d_work, nullptr);
+  s.fft1 = 1;
+  s.post = PW_LZ_X;
+  s.partial = p->d_partial;
+  TRY(sweep(p, AX_X, s, st));
+  s = mk_sweep(p->d_work, nullptr);
+  s.fft1 = 1;
+  s.post = PW_LZ_Y;
+  s.partial = p->d_partial + 4 * (size_t)p->max_tiles;
+  TRY(sweep(p, AX_Y, s, st));
+  const int nx = tiles_of(p, AX_X), ny = tiles_of(p, AX_Y);
+  std::vector<double> hx(4 * (size_t)nx), hy(4 * (size_t)ny);
+  CU(cudaMemcpyAsync(hx.data(), p->d_partial, hx.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(hy.data(), p->d_partial + 4 * (size_t)p->max_tiles, hy.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  // compensated sums in tile order
+  auto csum = [](const std::vector<double>& v, int count) {
+    double sum = 0.0, c = 0.0;
+    for (int b = 0; b < count; ++b) {
+      const double y = v[4 * (size_t)b + 3] - c, t = sum + y;
+      c = (t - sum) - y;
+      sum = t;
+    }
+    return sum;
+  };
+  const double n2 = (double)p->n * p->n;
+  *lz = (csum(hy, ny) - csum(hx, nx)) / n2 * p->ph.dx3;
+  return GPE_OK;
+}
+
 // {N, E_kin, E_pot, E_int, E, mu} from the finished sums h[0..3].
 void diag_scalars(const gpe_plan* p, const double* h, double* scalars) {
   const double dx3 = p->ph.dx3;
@@ -1004,6 +1045,11 @@ int gpe_profile_read(gpe_plan* p, double* ms, long long* count) {
     count[r.ax] += 1;
   }
   return GPE_OK;
+}
+
+int gpe_angular_momentum(gpe_plan* p, const void* psi, double* lz, void* stream) {
+  if (!p || !psi || !lz) return fail(GPE_ERR_ARG, "null argument");
+  return angular_momentum(p, psi, lz, (cudaStream_t)stream);
 }
 
 int gpe_status(gpe_plan* p, int* flags, void* stream) {

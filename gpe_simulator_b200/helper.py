@@ -68,6 +68,13 @@ def get_E(psi_k, x_array, k_array):
     return utility_plan(psi_k, x_array, k_array).kinetic_energy(psi_k)
 
 
+def get_L(psi, x_array, k_array, slab_size=16):
+    """``gpe/helper.py:143-156``: ``Lz = Re integral psi* (x p_y - y p_x) psi dV`` with
+    spectral momenta (``slab_size`` is accepted for the reference's signature; the
+    sums here need no slabs)."""
+    return utility_plan(psi, x_array, k_array).angular_momentum(psi)
+
+
 def get_beta(N_atoms, a):
     """``gpe/helper.py:109-113`` (a in Bohr radii, l = 1 micrometre)."""
     return 8 * math.pi * N_atoms * (a * 5.29177210544e-11) / 1e-6

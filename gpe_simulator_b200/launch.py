@@ -47,6 +47,8 @@ def launch_stage(stage, on_diagnostics=None):
         if want_scalar or want_nk:
             plan, psi = prop.binding.plan(stage)
             rec = plan.diagnostics(psi, t=i * stage.dt, nk=want_nk)
+            if want_scalar:
+                rec["Lz"] = plan.angular_momentum(psi)
             rec.update(step=i, time=i * stage.dt)
             history.append(rec)
             _write(stage, rec, want_scalar, want_nk)
@@ -68,9 +70,10 @@ def _write(stage, rec, scalar, nk):
         with path.open("a", newline="") as f:
             w = csv.writer(f)
             if new:
-                w.writerow(["step", "time", "norm", "N_atoms", "E_kin", "E", "mu"])
+                # the reference's columns (gpe/save.py:53), then total energy and mu
+                w.writerow(["step", "time", "norm", "N_atoms", "E_kin", "Lz", "E", "mu"])
             w.writerow([rec["step"], rec["time"], rec["N"], stage.N_atoms * rec["N"], rec["E_kin"],
-                        rec["E"], rec["mu"]])
+                        rec["Lz"], rec["E"], rec["mu"]])
     if nk:
         np.savez(folder / f"nk_{rec['step']:08d}.npz", step=rec["step"], time=rec["time"],
                  Nk=rec["Nk"], counts=rec["counts"])

@@ -207,6 +207,13 @@ class Plan:
         _lib.check(self.lib.gpe_kinetic_energy(self._h, p, ctypes.byref(out), _stream()))
         return out.value
 
+    def angular_momentum(self, psi):
+        """Lz of ``psi`` (``gpe/helper.py:143-156``), FP64 sums."""
+        p = self._check(psi)
+        out = ctypes.c_double()
+        _lib.check(self.lib.gpe_angular_momentum(self._h, p, ctypes.byref(out), _stream()))
+        return out.value
+
     def shells(self, psi_k):
         """``(Nk, counts)`` per shell of a spectrum."""
         p = self._check(psi_k, "psi_k")

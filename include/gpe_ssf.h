@@ -156,6 +156,11 @@ int  gpe_nk_extraction(gpe_plan* plan, const void* psi_k, double* occupation,
 int  gpe_diagnostics(gpe_plan* plan, const void* psi, double t, double* scalars,
                      double* nk, long long* counts, void* stream);
 
+/* Lz = Re integral psi* (x p_y - y p_x) psi dV with spectral momenta (reference
+ * gpe/helper.py:143-156 get_L); three sweeps through the plan's work buffer,
+ * synchronises `stream` */
+int  gpe_angular_momentum(gpe_plan* plan, const void* psi, double* lz, void* stream);
+
 /* accounting: kernel launches issued by this plan since creation */
 int  gpe_launch_count(const gpe_plan* plan, long long* count);
 /* per-launch timing: enable = 1 brackets every sweep launch with CUDA events on its

@@ -248,6 +248,21 @@ def get_E(psi_k, x, k):
     return float(np.sum(np.abs(psi_k.astype(np.complex128)) ** 2 * k2)) * dx ** 3 / psi_k.size
 
 
+def get_L(psi, x, k, slab_size=16):
+    """``gpe/helper.py:143-156``: ``Lz = dx^3 sum [x Re(psi* P_y psi) - y Re(psi* P_x psi)]``
+    with spectral momenta ``P = ifftn(k fftn(.))`` over the (x, y) axes of z slabs."""
+    dx = x[1] - x[0]
+    L = 0.0
+    for start in range(0, psi.shape[2], slab_size):
+        slab = psi[:, :, start:start + slab_size].astype(np.complex128)
+        sk = np.fft.fftn(slab, axes=(0, 1))
+        my = np.fft.ifftn(sk * k[None, :, None], axes=(0, 1))
+        L += float(np.sum(x[:, None, None] * (slab.real * my.real + slab.imag * my.imag)))
+        mx = np.fft.ifftn(sk * k[:, None, None], axes=(0, 1))
+        L -= float(np.sum(x[None, :, None] * (slab.real * mx.real + slab.imag * mx.imag)))
+    return L * dx ** 3
+
+
 def reference_nbins(n):
     """``gpe/nk_extraction.py:21``."""
     return int(math.floor(math.sqrt(3) * (n // 2) + 0.5)) + 1

@@ -22,7 +22,7 @@ are regenerated from the stored seeds, so the fixtures hold outputs only:
   Gamma`` ramp plus a real box) and a momentum cutoff, N=16.
 * ``box24``      imaginary time with a float64 box potential array plus a
   static expression, N=24.
-* ``diag_n*``    ``get_N``, ``get_E`` and ``nk_extraction`` of seeded states.
+* ``diag_n*``    ``get_N``, ``get_E``, ``get_L`` and ``nk_extraction`` of seeded states.
 
 Usage: ``python tests/golden/make_golden.py`` (writes ``tests/golden/*.npz``).
 """
@@ -123,8 +123,8 @@ def make_diag(ref):
         F = np.fft.fftn(psi)
         spec = ref.nk_extraction.nk_extraction(F, x, k, slab_size=3)
         save(f"diag_n{n}", N=float(ref.helper.get_N(psi, x)),
-             E_kin=float(ref.helper.get_E(F, x, k)), **{f"nk_{key}": np.asarray(val)
-                                                      for key, val in spec.items()})
+             E_kin=float(ref.helper.get_E(F, x, k)), L=float(ref.helper.get_L(psi, x, k, slab_size=3)),
+             **{f"nk_{key}": np.asarray(val) for key, val in spec.items()})
 
 
 def main(which=None):

@@ -131,3 +131,5 @@ def test_stage_run_logs_norm_and_energy_every_50_steps(tmp_path):
     assert all(np.isfinite(h["E"]) for h in hist)
     rows = (tmp_path / "scalars.csv").read_text().strip().splitlines()
     assert len(rows) == 1 + 100
+    assert rows[0].split(",")[:6] == ["step", "time", "norm", "N_atoms", "E_kin", "Lz"]
+    assert all(np.isfinite(h["Lz"]) for h in hist)

@@ -141,3 +141,18 @@ def test_diagnostics_match_reference(cuda, n, L):
     np.testing.assert_array_equal(spec["edges"], g["nk_edges"])
     np.testing.assert_array_equal(spec["k"], g["nk_k"])
     np.testing.assert_array_equal(spec["complete_shells"], g["nk_complete_shells"])
+    # angular momentum: the reference's get_L on the same state
+    assert helper.get_L(psi, x, k) == pytest.approx(float(g["L"]), rel=1e-10, abs=1e-10)
+
+
+@pytest.mark.parametrize("charge", [-1, 1])
+@pytest.mark.parametrize("dtype,rel", [(torch.complex128, 1e-9), (torch.complex64, 2e-5)])
+def test_vortex_angular_momentum(cuda, charge, dtype, rel):
+    """``tests/test_diagnostics.py:40-48``: a charge-q vortex carries Lz = q N."""
+    from gpe_simulator_b200 import helper
+    x, k = helper.get_grids(48, 16.0)
+    xs = x.cpu().numpy()
+    X, Y, Z = xs[:, None, None], xs[None, :, None], xs[None, None, :]
+    psi = torch.from_numpy((X + charge * 1j * Y) * np.exp(-(X * X + Y * Y + Z * Z) / 2)).to(dtype).cuda()
+    N = helper.get_N(psi, x)
+    assert helper.get_L(psi, x, k, slab_size=7) == pytest.approx(charge * N, rel=rel, abs=1e-10)

@@ -95,6 +95,18 @@ def test_diagnostics_against_reference_fixtures(n, L):
     # Parseval (``tests/test_diagnostics.py:52-72``)
     assert spec["Nk"].sum() == pytest.approx(ssf.get_N(psi, x), rel=1e-12)
     assert spec["counts"].sum() == n ** 3
+    # angular momentum (reference get_L, slab size 3 in the fixture; the sum is slab-independent)
+    assert ssf.get_L(psi, x, k, slab_size=5) == pytest.approx(float(g["L"]), rel=1e-11, abs=1e-11)
+
+
+@pytest.mark.parametrize("charge", [-1, 1])
+def test_vortex_angular_momentum(charge):
+    """``tests/test_diagnostics.py:40-48``: a charge-q vortex carries Lz = q N."""
+    x, k = ssf.get_grids(48, 16.0)
+    X, Y, Z = x[:, None, None], x[None, :, None], x[None, None, :]
+    psi = (X + charge * 1j * Y) * np.exp(-(X * X + Y * Y + Z * Z) / 2)
+    N = ssf.get_N(psi, x)
+    assert ssf.get_L(psi, x, k, slab_size=7) == pytest.approx(charge * N, rel=1e-9, abs=1e-10)
 
 
 def test_ground_state_fixture_first_checkpoint():
