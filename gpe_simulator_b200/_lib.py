@@ -61,6 +61,7 @@ SIGNATURES = {
     "gpe_diagnostics": [_vp, _vp, ctypes.c_double, _dp, _dp, _llp, _vp],
     "gpe_status": [_vp, ctypes.POINTER(ctypes.c_int), _vp],
     "gpe_angular_momentum": [_vp, _vp, _dp, _vp],
+    "gpe_projections": [_vp, _vp, ctypes.c_uint, _dp, _vp],
     "gpe_launch_count": [_vp, _llp],
     "gpe_profile": [_vp, ctypes.c_int],
     "gpe_profile_read": [_vp, _dp, _llp],

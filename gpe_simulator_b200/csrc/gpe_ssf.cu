@@ -206,6 +206,71 @@ __global__ void k_finish_diag_batch(const DiagJob* jobs, double* out) {
     for (int v = 0; v < 4; ++v) out[4 * j.index + v] = a[v].value();
 }
 
+// ---------------------------------------------------------------- image projections
+// The image outputs of the reference's save_outputs (gpe/save.py:59-90); out
+// arrays are n x n, row-major, at fftshifted indices for the momentum images.
+__device__ __forceinline__ int fftshift_index(int i, int n) { return (i + n / 2) % n; }
+
+// one warp per (a, b) line along the contiguous axis: sum |v|^2 over it, and the
+// element at `pick` of the line; `shift` selects fftshifted output indices
+template <typename C>
+__global__ void k_proj_lines(const C* __restrict__ f, int n, double col_scale, double pick_scale, int pick,
+                             bool shift, double* __restrict__ col, double* __restrict__ sel,
+                             double* __restrict__ sel_phase) {
+  const long long line = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  const int lane = threadIdx.x & 31;
+  if (line >= (long long)n * n) return;
+  const int a = (int)(line / n), b = (int)(line % n);
+  const C* row = f + line * n;
+  double s = 0.0;
+  for (int z = lane; z < n; z += 32) s += (double)row[z].x * row[z].x + (double)row[z].y * row[z].y;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) {
+    const long long o = shift ? (long long)fftshift_index(a, n) * n + fftshift_index(b, n) : line;
+    if (col) col[o] = s * col_scale;
+    const C v = row[pick];
+    if (sel) sel[o] = ((double)v.x * v.x + (double)v.y * v.y) * pick_scale;
+    if (sel_phase) sel_phase[o] = atan2((double)v.y, (double)v.x);
+  }
+}
+
+// one thread per (b, c): sum |f[a][b][c]|^2 over the slowest axis a, and a = 0
+template <typename C>
+__global__ void k_proj_slow(const C* __restrict__ f, int n, double col_scale, double pick_scale,
+                            double* __restrict__ col, double* __restrict__ sel) {
+  const long long bc = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (bc >= (long long)n * n) return;
+  const long long plane = (long long)n * n;
+  double s = 0.0;
+  for (int a = 0; a < n; ++a) {
+    const C v = f[a * plane + bc];
+    s += (double)v.x * v.x + (double)v.y * v.y;
+  }
+  const int b = (int)(bc / n), c = (int)(bc % n);
+  const long long o = (long long)fftshift_index(b, n) * n + fftshift_index(c, n);
+  if (col) col[o] = s * col_scale;
+  if (sel) { const C v = f[bc]; sel[o] = ((double)v.x * v.x + (double)v.y * v.y) * pick_scale; }
+}
+
+// phase = NaN where the slice density is below 1e-12 of its maximum (one block)
+__global__ void k_phase_mask(const double* __restrict__ dens, double* __restrict__ phase, long long count) {
+  __shared__ double sm[32];
+  double m = 0.0;
+  for (long long i = threadIdx.x; i < count; i += blockDim.x) m = fmax(m, dens[i]);
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x / 32] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < blockDim.x / 32 ? sm[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) sm[0] = m;
+  }
+  __syncthreads();
+  const double thr = sm[0] * 1e-12;
+  for (long long i = threadIdx.x; i < count; i += blockDim.x)
+    if (!(dens[i] > thr)) phase[i] = nan("");
+}
+
 }  // namespace gpe
 
 // ---------------------------------------------------------------- the plan
@@ -244,6 +309,7 @@ struct gpe_plan {
   double* d_hist = nullptr;
   double* d_out = nullptr;       // diag results [4 + nbins]
   void* d_work = nullptr;        // diagnostic FFT scratch (size of psi), lazily
+  double* d_proj = nullptr;      // image projections: 7 n x n arrays, lazily
   int max_tiles = 0;
   // launch accounting and optional per-launch timing (events around each sweep)
   long long launches = 0;
@@ -563,7 +629,7 @@ void free_plan(gpe_plan* p) {
   for (auto e : p->pool) cudaEventDestroy(e);
   void* bufs[] = {p->d_x, p->d_k, p->d_kin, p->d_kth, p->d_vax, p->d_vre, p->d_vim, p->d_prog_g, p->d_dyn,
                   p->d_tw, p->d_partial, p->d_ticket, p->d_scale, p->d_status, p->d_hist, p->d_out,
-                  p->d_work, p->d_plane};
+                  p->d_work, p->d_plane, p->d_proj};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete p;
@@ -822,6 +888,48 @@ int angular_momentum(gpe_plan* p, const void* psi, double* lz, cudaStream_t st) 
   return GPE_OK;
 }
 
+// The selected image projections of psi (GPE_PROJ_* bits, reference
+// gpe/save.py:59-90) into `out` (host), n*n doubles per selected image in bit order.
+template <typename R>
+int projections(gpe_plan* p, const void* psi, unsigned which, double* out, cudaStream_t st) {
+  using C = typename Cx<R>::T;
+  const int n = p->n;
+  const long long nn = (long long)n * n;
+  if (!p->d_proj) CU(cudaMalloc(&p->d_proj, 7 * nn * sizeof(double)));
+  double* img[7];
+  for (int i = 0; i < 7; ++i) img[i] = (which >> i) & 1u ? p->d_proj + i * nn : nullptr;
+  const double dx = p->dx, dk = std::fabs(p->k[1] - p->k[0]);
+  const double scale = dx * dx * dx / ((double)nn * n * dk * dk * dk);
+  const unsigned tof = GPE_PROJ_TOF_XY | GPE_PROJ_TOF_YZ | GPE_PROJ_TOF_SLICE_XY | GPE_PROJ_TOF_SLICE_YZ;
+  const int warps_per_block = 8;
+  const unsigned lines_grid = (unsigned)((nn + warps_per_block - 1) / warps_per_block);
+  if (which & tof) {
+    TRY(ensure_work(p));
+    TRY(fft3d(p, psi, p->d_work, false, st));
+    const C* f = (const C*)p->d_work;
+    if (img[0] || img[2])
+      k_proj_lines<C><<<lines_grid, 32 * warps_per_block, 0, st>>>(f, n, scale * dk, scale, 0, true, img[0],
+                                                                   img[2], nullptr);
+    if (img[1] || img[3])
+      k_proj_slow<C><<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(f, n, scale * dk, scale, img[1], img[3]);
+    CU(cudaGetLastError());
+  }
+  if (which & (GPE_PROJ_DENSITY_XY | GPE_PROJ_DENSITY_SLICE_XY | GPE_PROJ_PHASE_XY)) {
+    double* slice = img[5] ? img[5] : (img[6] ? p->d_proj + 5 * nn : nullptr);
+    k_proj_lines<C><<<lines_grid, 32 * warps_per_block, 0, st>>>((const C*)psi, n, dx, 1.0, n / 2, false, img[4],
+                                                                 slice, img[6]);
+    if (img[6]) k_phase_mask<<<1, 1024, 0, st>>>(slice, img[6], nn);
+    CU(cudaGetLastError());
+  }
+  for (int i = 0, o = 0; i < 7; ++i)
+    if (img[i]) {
+      CU(cudaMemcpyAsync(out + (size_t)o * nn, img[i], nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+      ++o;
+    }
+  CU(cudaStreamSynchronize(st));
+  return GPE_OK;
+}
+
 // {N, E_kin, E_pot, E_int, E, mu} from the finished sums h[0..3].
 void diag_scalars(const gpe_plan* p, const double* h, double* scalars) {
   const double dx3 = p->ph.dx3;
@@ -1045,6 +1153,14 @@ int gpe_profile_read(gpe_plan* p, double* ms, long long* count) {
     count[r.ax] += 1;
   }
   return GPE_OK;
+}
+
+int gpe_projections(gpe_plan* p, const void* psi, unsigned which, double* out, void* stream) {
+  if (!p || !psi || (which && !out)) return fail(GPE_ERR_ARG, "null argument");
+  if (which >> 7) return fail(GPE_ERR_ARG, "unknown projection bits");
+  cudaStream_t st = (cudaStream_t)stream;
+  return p->dtype == GPE_C64 ? projections<float>(p, psi, which, out, st)
+                             : projections<double>(p, psi, which, out, st);
 }
 
 int gpe_angular_momentum(gpe_plan* p, const void* psi, double* lz, void* stream) {

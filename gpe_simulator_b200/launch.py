@@ -16,18 +16,26 @@ import numpy as np
 from .helper import is_due
 
 
+# monitor interval -> image outputs it asks for (gpe/save.py:59-90)
+_IMAGES = {"show_TOF_image_interval": ("TOF_xy",), "show_verticle_TOF_interval": ("TOF_yz",),
+           "show_TOF_slice_interval": ("TOF_slice_xy",), "show_verticle_TOF_slice_interval": ("TOF_slice_yz",),
+           "show_magnifier_interval": ("density_xy",), "show_magnifier_slice_interval": ("density_slice_xy",),
+           "show_phase_interval": ("phase_xy",)}
+
+
 def _due_steps(stage):
     save = getattr(stage, "save_params", None) or {}
     monitor = getattr(stage, "monitor_params", None) or {}
     scalar = [save.get("scalar_interval"), monitor.get("print_scalar_interval")]
     spectrum = [save.get("nk_interval"), monitor.get("show_nk_interval")]
-    return scalar, spectrum
+    images = {key: monitor.get(key) for key in _IMAGES}
+    return scalar, spectrum, images
 
 
 def launch_stage(stage, on_diagnostics=None):
     """Run a prepared stage and return its final wavefunction (``stage.psi``)."""
-    scalar, spectrum = _due_steps(stage)
-    intervals = [i for i in scalar + spectrum if i]
+    scalar, spectrum, images = _due_steps(stage)
+    intervals = [i for i in scalar + spectrum + list(images.values()) if i]
     prop = stage.propagator
     history = []
     i = 0
@@ -44,6 +52,10 @@ def launch_stage(stage, on_diagnostics=None):
         i = stop
         want_scalar = any(is_due(i, iv) for iv in scalar)
         want_nk = any(is_due(i, iv) for iv in spectrum)
+        want_img = [name for key, iv in images.items() if is_due(i, iv) for name in _IMAGES[key]]
+        if want_img:
+            plan, psi = prop.binding.plan(stage)
+            _write_images(stage, i, plan.projections(psi, want_img))
         if want_scalar or want_nk:
             plan, psi = prop.binding.plan(stage)
             rec = plan.diagnostics(psi, t=i * stage.dt, nk=want_nk)
@@ -56,6 +68,25 @@ def launch_stage(stage, on_diagnostics=None):
                 on_diagnostics(stage, rec)
     stage.history = history
     return stage.psi
+
+
+def _write_images(stage, step, images):
+    """The reference's image files (``gpe/save.py:59-90``): ``<name>_<step>.npz``
+    with ``step``, ``time``, ``values`` and the axes."""
+    folder = getattr(stage, "monitor_dir", None)
+    if folder is None:
+        return
+    folder = Path(folder)
+    folder.mkdir(parents=True, exist_ok=True)
+    x = stage.x_array.detach().cpu().numpy() if hasattr(stage.x_array, "detach") else np.asarray(stage.x_array)
+    k = stage.k_array.detach().cpu().numpy() if hasattr(stage.k_array, "detach") else np.asarray(stage.k_array)
+    ks = np.fft.fftshift(k)
+    mid = stage.N_grids // 2
+    axes = {"TOF_xy": dict(kx=ks, ky=ks), "TOF_yz": dict(ky=ks, kz=ks), "TOF_slice_xy": dict(kx=ks, ky=ks),
+            "TOF_slice_yz": dict(ky=ks, kz=ks), "density_xy": dict(x=x, y=x),
+            "density_slice_xy": dict(x=x, y=x, z=x[mid]), "phase_xy": dict(x=x, y=x, z=x[mid])}
+    for name, values in images.items():
+        np.savez(folder / f"{name}_{step:08d}.npz", step=step, time=step * stage.dt, values=values, **axes[name])
 
 
 def _write(stage, rec, scalar, nk):

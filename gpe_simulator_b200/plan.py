@@ -214,6 +214,23 @@ class Plan:
         _lib.check(self.lib.gpe_angular_momentum(self._h, p, ctypes.byref(out), _stream()))
         return out.value
 
+    PROJECTIONS = ("TOF_xy", "TOF_yz", "TOF_slice_xy", "TOF_slice_yz", "density_xy", "density_slice_xy",
+                   "phase_xy")
+
+    def projections(self, psi, which=None):
+        """Image outputs of ``gpe/save.py:59-90`` as ``{name: (n, n) array}``; ``which``
+        is an iterable of names from :attr:`PROJECTIONS` (default: all)."""
+        names = list(self.PROJECTIONS if which is None else which)
+        bits = 0
+        for name in names:
+            bits |= 1 << self.PROJECTIONS.index(name)
+        p = self._check(psi)
+        chosen = [nm for nm in self.PROJECTIONS if bits >> self.PROJECTIONS.index(nm) & 1]
+        out = np.empty((len(chosen), self.n, self.n))
+        _lib.check(self.lib.gpe_projections(self._h, p, bits, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                            _stream()))
+        return dict(zip(chosen, out))
+
     def shells(self, psi_k):
         """``(Nk, counts)`` per shell of a spectrum."""
         p = self._check(psi_k, "psi_k")

@@ -161,6 +161,20 @@ int  gpe_diagnostics(gpe_plan* plan, const void* psi, double t, double* scalars,
  * synchronises `stream` */
 int  gpe_angular_momentum(gpe_plan* plan, const void* psi, double* lz, void* stream);
 
+/* Image outputs of the reference's save_outputs (gpe/save.py:59-90): bits select
+ * the images; `out` (host) receives n*n doubles (row-major) per selected image,
+ * in bit order.  Momentum images are of |fftn(psi)|^2, fftshifted, scaled by
+ * dx^3/(M dk^3) (the column sums also by dk); the phase is NaN where the z = n/2
+ * slice density is below 1e-12 of its maximum.  Synchronises `stream`. */
+#define GPE_PROJ_TOF_XY           1u   /* sum over kz */
+#define GPE_PROJ_TOF_YZ           2u   /* sum over kx */
+#define GPE_PROJ_TOF_SLICE_XY     4u   /* kz = 0 */
+#define GPE_PROJ_TOF_SLICE_YZ     8u   /* kx = 0 */
+#define GPE_PROJ_DENSITY_XY      16u   /* dx * sum over z of |psi|^2 */
+#define GPE_PROJ_DENSITY_SLICE_XY 32u  /* |psi|^2 at z = n/2 */
+#define GPE_PROJ_PHASE_XY        64u   /* arg psi at z = n/2 */
+int  gpe_projections(gpe_plan* plan, const void* psi, unsigned which, double* out, void* stream);
+
 /* accounting: kernel launches issued by this plan since creation */
 int  gpe_launch_count(const gpe_plan* plan, long long* count);
 /* per-launch timing: enable = 1 brackets every sweep launch with CUDA events on its

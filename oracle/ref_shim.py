@@ -289,16 +289,27 @@ class HostReductionKernel:
         self._lib = _compile("red_" + self.name, src)
 
     def __call__(self, *args, axis=None):
-        assert axis is None, "only full reductions are used on the propagator path"
         if self._lib is None:
             self._build()
         ins = [np.asarray(a) for a in args[:len(self.ins)]]
         shape = np.broadcast_shapes(*[a.shape for a in ins])
         flat = [np.ascontiguousarray(np.broadcast_to(a.astype(_NP[t], copy=False), shape))
                 for a, (t, _) in zip(ins, self.ins)]
-        out = np.zeros((), _NP[self.outs[0][0]])
-        self._lib.red(ctypes.c_longlong(int(np.prod(shape))),
-                      *[ctypes.c_void_p(a.ctypes.data) for a in flat + [out]])
+        otype = _NP[self.outs[0][0]]
+        if axis is None:
+            out = np.zeros((), otype)
+            self._lib.red(ctypes.c_longlong(int(np.prod(shape))),
+                          *[ctypes.c_void_p(a.ctypes.data) for a in flat + [out]])
+            return out
+        # reduction along one axis: the same sequential loop over every line
+        lines = [np.ascontiguousarray(np.moveaxis(a, axis, -1)) for a in flat]
+        out = np.zeros(lines[0].shape[:-1], otype)
+        cell = np.zeros((), otype)
+        for idx in np.ndindex(out.shape):
+            line = [np.ascontiguousarray(a[idx]) for a in lines]
+            self._lib.red(ctypes.c_longlong(line[0].shape[0]),
+                          *[ctypes.c_void_p(a.ctypes.data) for a in line + [cell]])
+            out[idx] = cell
         return out
 
 
@@ -321,7 +332,7 @@ def install():
         sys.path.insert(0, str(REFERENCE))
     mods = {name: importlib.import_module("gpe." + name)
             for name in ("make_propagator", "make_kernel", "kernels", "helper",
-                         "nk_extraction", "grids", "initial_states", "expressions")}
+                         "nk_extraction", "grids", "initial_states", "expressions", "save")}
     return SimpleNamespace(cp=cupy, **mods)
 
 

@@ -263,6 +263,35 @@ def get_L(psi, x, k, slab_size=16):
     return L * dx ** 3
 
 
+PROJECTIONS = ("TOF_xy", "TOF_yz", "TOF_slice_xy", "TOF_slice_yz", "density_xy", "density_slice_xy",
+               "phase_xy")
+
+
+def projections(psi, x, k):
+    """The image outputs of ``gpe/save.py:59-90`` (values only): momentum-space
+    (time-of-flight) column sums over z and x and the kz = 0 / kx = 0 slices of
+    ``|fftn(psi)|^2``, fftshifted and scaled by ``dx^3/(M dk^3)`` (columns also by
+    ``dk``); the real-space column density over z (times dx), the z = N/2 slice
+    of ``|psi|^2`` and its phase (NaN where the slice density is below 1e-12 of
+    its maximum)."""
+    psi = psi.astype(np.complex128)
+    n = psi.shape[0]
+    dx = float(x[1] - x[0])
+    dk = abs(float(k[1] - k[0]))
+    F = np.fft.fftn(psi)
+    w = np.abs(F) ** 2
+    scale = dx ** 3 / (psi.size * dk ** 3)
+    sh = np.fft.fftshift
+    out = dict(TOF_xy=sh(w.sum(axis=2)) * (scale * dk), TOF_yz=sh(w.sum(axis=0)) * (scale * dk),
+               TOF_slice_xy=sh(w[:, :, 0]) * scale, TOF_slice_yz=sh(w[0, :, :]) * scale)
+    out["density_xy"] = (np.abs(psi) ** 2).sum(axis=2) * dx
+    plane = psi[:, :, n // 2]
+    dens = np.abs(plane) ** 2
+    out["density_slice_xy"] = dens
+    out["phase_xy"] = np.where(dens > dens.max() * 1e-12, np.angle(plane), np.nan)
+    return out
+
+
 def reference_nbins(n):
     """``gpe/nk_extraction.py:21``."""
     return int(math.floor(math.sqrt(3) * (n // 2) + 0.5)) + 1

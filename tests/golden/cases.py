@@ -26,6 +26,7 @@ BOX24 = dict(n=24, L=12.0, beta=150.0, dt=1e-3, static_expr="0.2*(x*x+y*y)", see
              steps=100, R=3.0, length=8.0, wall=0.5, depth=10.0)
 
 DIAG_SIZES = ((2, 2 * np.pi), (7, 2 * np.pi), (8, 2 * np.pi), (18, 2 * np.pi), (32, 10.0))
+PROJ_SIZES = ((16, 8.0), (15, 6.0))
 
 
 def stir_beam():

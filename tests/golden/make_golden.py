@@ -23,6 +23,8 @@ are regenerated from the stored seeds, so the fixtures hold outputs only:
 * ``box24``      imaginary time with a float64 box potential array plus a
   static expression, N=24.
 * ``diag_n*``    ``get_N``, ``get_E``, ``get_L`` and ``nk_extraction`` of seeded states.
+* ``proj_n*``    the image outputs of ``save_outputs`` (TOF columns and slices, column
+                 density, density slice and phase) of seeded states.
 
 Usage: ``python tests/golden/make_golden.py`` (writes ``tests/golden/*.npz``).
 """
@@ -127,9 +129,35 @@ def make_diag(ref):
              **{f"nk_{key}": np.asarray(val) for key, val in spec.items()})
 
 
+def make_proj(ref):
+    """The reference's own save_outputs (``gpe/save.py:59-90``) with every image
+    output due, on seeded states (even and odd n: fftshift)."""
+    import tempfile
+    from types import SimpleNamespace
+    for n, L in cases.PROJ_SIZES:
+        x, k = ref.grids.get_grids(n, L)
+        psi = cases.diag_state(n, seed=7)
+        with tempfile.TemporaryDirectory() as tmp:
+            monitor = {name: 1 for name in ("show_TOF_image_interval", "show_verticle_TOF_interval",
+                                            "show_TOF_slice_interval", "show_verticle_TOF_slice_interval",
+                                            "show_magnifier_interval", "show_magnifier_slice_interval",
+                                            "show_phase_interval")}
+            monitor.update(print_scalar_interval=None, show_nk_interval=None)
+            st = SimpleNamespace(save_params=dict(psi_interval=None, save_initial=False, save_final=False,
+                                                  scalar_interval=None, nk_interval=None),
+                                 monitor_params=monitor, monitor_dir=Path(tmp), psi=psi, x_array=x,
+                                 k_array=k, N_grids=n, dt=0.1, name="proj")
+            ref.save.save_outputs(st, 1)
+            files = {"TOF_xy": "TOF_xy", "TOF_yz": "TOF_yz", "TOF_slice_xy": "TOF_slice_xy",
+                     "TOF_slice_yz": "TOF_slice_yz", "density_xy": "density_xy",
+                     "density_slice_xy": "density_slice_xy", "phase_xy": "phase_xy"}
+            vals = {key: np.load(Path(tmp) / f"{name}_00000001.npz")["values"] for key, name in files.items()}
+        save(f"proj_n{n}", **vals)
+
+
 def main(which=None):
     ref = ref_shim.install()
-    jobs = dict(diag=make_diag, lossy16=make_lossy16, box24=make_box24,
+    jobs = dict(diag=make_diag, proj=make_proj, lossy16=make_lossy16, box24=make_box24,
                 stir32=make_stir32, ground64=make_ground64)
     for name, job in jobs.items():
         if which is None or name in which:

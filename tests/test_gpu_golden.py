@@ -156,3 +156,58 @@ def test_vortex_angular_momentum(cuda, charge, dtype, rel):
     psi = torch.from_numpy((X + charge * 1j * Y) * np.exp(-(X * X + Y * Y + Z * Z) / 2)).to(dtype).cuda()
     N = helper.get_N(psi, x)
     assert helper.get_L(psi, x, k, slab_size=7) == pytest.approx(charge * N, rel=rel, abs=1e-10)
+
+
+@pytest.mark.parametrize("n,L", cases.PROJ_SIZES)
+@pytest.mark.parametrize("dtype,rtol", [(torch.complex128, 1e-12), (torch.complex64, 2e-6)])
+def test_projections_match_reference_save_outputs(cuda, n, L, dtype, rtol):
+    """TOF columns and slices, column density, density slice and phase images as
+    the reference's save_outputs writes them (even and odd n for fftshift)."""
+    from gpe_simulator_b200 import Plan
+    g = load(f"proj_n{n}")
+    x, k = ssf.get_grids(n, L)
+    plan = Plan(n, x, k, dtype=dtype, kind="imaginary", beta=0.0, dt=0.0)
+    psi = torch.from_numpy(cases.diag_state(n, seed=7)).to(dtype).cuda()
+    out = plan.projections(psi)
+    assert list(out) == list(ssf.PROJECTIONS)
+    for key in ssf.PROJECTIONS:
+        want = g[key]
+        np.testing.assert_array_equal(np.isnan(out[key]), np.isnan(want), err_msg=key)
+        scale = np.nanmax(np.abs(want))
+        np.testing.assert_allclose(np.nan_to_num(out[key]), np.nan_to_num(want), rtol=rtol,
+                                   atol=(1e-12 if dtype == torch.complex128 else 2e-6) * scale, err_msg=key)
+    sub = plan.projections(psi, ["phase_xy", "TOF_yz"])
+    assert list(sub) == ["TOF_yz", "phase_xy"]
+    assert np.array_equal(sub["TOF_yz"], out["TOF_yz"], equal_nan=True)
+
+
+def test_stage_writes_reference_image_files(cuda, tmp_path):
+    """launch_stage writes the reference's image files when their intervals are due."""
+    from gpe_simulator_b200 import helper
+    from gpe_simulator_b200.expressions import cuda_expression
+    from gpe_simulator_b200.launch import launch_stage
+    from gpe_simulator_b200.stage import stage
+    n, L = 16, 8.0
+    x, k = helper.get_grids(n, L)
+    monitor = {key: 2 for key in ("show_TOF_image_interval", "show_verticle_TOF_interval",
+                                  "show_TOF_slice_interval", "show_verticle_TOF_slice_interval",
+                                  "show_magnifier_interval", "show_magnifier_slice_interval",
+                                  "show_phase_interval")}
+    st = stage(simulation_range=L, x_array=x, k_array=k, N_grids=n, type="imaginary", steps=4, dt=1e-3,
+               initial_state=dict(type="gaussian", sigma=1.0), box_params=dict(activate=False),
+               absorber_params=dict(activate=False), noise_params=dict(activate=False),
+               cloud_params=dict(a=0.0, N_atom=1), monitor_params=monitor,
+               save_params=dict(scalar_interval=0, nk_interval=0),
+               potential_params=dict(static=dict(activate=True, expression=cuda_expression("x**2+y**2+z**2")),
+                                     dynamic=dict(activate=False, expression="0")),
+               k_cut_params=dict(activate=False, k_cut=0.0))
+    st.prepare()
+    st.monitor_dir = tmp_path
+    psi = launch_stage(st)
+    for name in ssf.PROJECTIONS:
+        files = sorted(tmp_path.glob(f"{name}_*.npz"))
+        assert [f.name for f in files] == [f"{name}_00000002.npz", f"{name}_00000004.npz"], name
+    f = np.load(tmp_path / "TOF_xy_00000004.npz")
+    want = ssf.projections(psi.cpu().numpy(), x.cpu().numpy(), k.cpu().numpy())["TOF_xy"]
+    np.testing.assert_allclose(f["values"], want, rtol=1e-10, atol=1e-14)
+    assert set(f.files) == {"step", "time", "values", "kx", "ky"}

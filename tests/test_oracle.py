@@ -184,3 +184,14 @@ def test_expression_evaluator_grammar():
     for bad in ("t*y", "x; 0", "foo(x)", "x^2"):
         with pytest.raises((ValueError, SyntaxError)):
             expr.evaluate(bad, X, 0, 0)
+
+
+@pytest.mark.parametrize("n,L", cases.PROJ_SIZES)
+def test_projections_against_reference_save_outputs(n, L):
+    """TOF and density images as the reference's save_outputs writes them."""
+    g = np.load(GOLD / f"proj_n{n}.npz")
+    x, k = ssf.get_grids(n, L)
+    out = ssf.projections(cases.diag_state(n, seed=7), x, k)
+    for key in ssf.PROJECTIONS:
+        np.testing.assert_array_equal(np.isnan(out[key]), np.isnan(g[key]))
+        np.testing.assert_allclose(np.nan_to_num(out[key]), np.nan_to_num(g[key]), rtol=1e-12, atol=1e-14)
