@@ -29,12 +29,24 @@ def _due_steps(stage):
     scalar = [save.get("scalar_interval"), monitor.get("print_scalar_interval")]
     spectrum = [save.get("nk_interval"), monitor.get("show_nk_interval")]
     images = {key: monitor.get(key) for key in _IMAGES}
+    images["psi_interval"] = save.get("psi_interval")
     return scalar, spectrum, images
+
+
+def _snapshot(stage, step):
+    """``psi_<step>.npy`` in the stage's data folder (``gpe/save.py:15-17``)."""
+    from .state_io import save_wavefunction
+    folder = getattr(stage, "data_dir", None)
+    if folder is not None:
+        save_wavefunction(Path(folder) / f"psi_{step:08d}.npy", stage, step)
 
 
 def launch_stage(stage, on_diagnostics=None):
     """Run a prepared stage and return its final wavefunction (``stage.psi``)."""
     scalar, spectrum, images = _due_steps(stage)
+    save = getattr(stage, "save_params", None) or {}
+    if save.get("save_initial"):
+        _snapshot(stage, 0)
     intervals = [i for i in scalar + spectrum + list(images.values()) if i]
     prop = stage.propagator
     history = []
@@ -52,7 +64,10 @@ def launch_stage(stage, on_diagnostics=None):
         i = stop
         want_scalar = any(is_due(i, iv) for iv in scalar)
         want_nk = any(is_due(i, iv) for iv in spectrum)
-        want_img = [name for key, iv in images.items() if is_due(i, iv) for name in _IMAGES[key]]
+        want_img = [name for key, iv in images.items() if key in _IMAGES and is_due(i, iv)
+                    for name in _IMAGES[key]]
+        if is_due(i, images["psi_interval"]) or (i == stage.steps and save.get("save_final")):
+            _snapshot(stage, i)
         if want_img:
             plan, psi = prop.binding.plan(stage)
             _write_images(stage, i, plan.projections(psi, want_img))

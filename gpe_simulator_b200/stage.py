@@ -118,10 +118,8 @@ class stage:  # noqa: N801 -- the reference's class name
                 raise ValueError("A continue stage needs the preceding stage's wavefunction.")
             return previous_psi.to(dtype).contiguous()
         if kind == "load":
-            saved = np.load(self.initial_state["path"], mmap_mode="r", allow_pickle=False)
-            if saved.shape != self._shape() or saved.dtype != np.complex128:
-                raise ValueError("The loaded state must be a complex128 cube matching N_grids.")
-            return torch.from_numpy(np.ascontiguousarray(saved)).to(self.x_array.device).to(dtype)
+            from .state_io import load_wavefunction
+            return load_wavefunction(self.initial_state["path"], self, dtype)
         if kind == "gaussian":
             return gaussian(self.x_array, self.initial_state["sigma"], dtype=dtype)
         raise ValueError(f"Unknown initial state: {kind}")

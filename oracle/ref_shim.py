@@ -321,6 +321,7 @@ def install():
     cupy.__getattr__ = lambda name: getattr(np, name)
     cupy.ndarray = np.ndarray
     cupy.asnumpy = np.asarray
+    cupy.asarray = lambda a, dtype=None, blocking=False, **kw: np.array(a, dtype=dtype)
     cupy.asarray = lambda value, blocking=False, **kw: np.asarray(value, **kw)
     cupy.fft = SimpleNamespace(fftn=np.fft.fftn, ifftn=np.fft.ifftn, fftfreq=np.fft.fftfreq,
                                fftshift=np.fft.fftshift)
@@ -332,7 +333,7 @@ def install():
         sys.path.insert(0, str(REFERENCE))
     mods = {name: importlib.import_module("gpe." + name)
             for name in ("make_propagator", "make_kernel", "kernels", "helper",
-                         "nk_extraction", "grids", "initial_states", "expressions", "save")}
+                         "nk_extraction", "grids", "initial_states", "expressions", "save", "state_io")}
     return SimpleNamespace(cp=cupy, **mods)
 
 

@@ -133,3 +133,31 @@ def test_stage_run_logs_norm_and_energy_every_50_steps(tmp_path):
     assert len(rows) == 1 + 100
     assert rows[0].split(",")[:6] == ["step", "time", "norm", "N_atoms", "E_kin", "Lz"]
     assert all(np.isfinite(h["Lz"]) for h in hist)
+
+
+def test_stage_snapshots_round_trip(tmp_path):
+    """launch_stage writes psi snapshots (complex128 files) at psi_interval and at
+    the end; a complex64 stage reloads the last one exactly."""
+    from gpe_simulator_b200 import helper
+    from gpe_simulator_b200.expressions import cuda_expression
+    from gpe_simulator_b200.launch import launch_stage
+    from gpe_simulator_b200.stage import stage
+
+    def make(initial):
+        x, k = helper.get_grids(32, 10.0)
+        return stage(simulation_range=10.0, x_array=x, k_array=k, N_grids=32, type="imaginary", steps=6,
+                     dt=1e-3, initial_state=initial, box_params=dict(activate=False),
+                     absorber_params=dict(activate=False), noise_params=dict(activate=False),
+                     cloud_params=dict(a=0.0, N_atom=1), monitor_params={},
+                     save_params=dict(scalar_interval=0, nk_interval=0, psi_interval=4, save_final=True),
+                     potential_params=dict(static=dict(activate=True, expression=cuda_expression("x**2+y**2+z**2")),
+                                           dynamic=dict(activate=False, expression="0")),
+                     k_cut_params=dict(activate=False, k_cut=0.0), precision="complex64")
+    st = make(dict(type="gaussian", sigma=1.0))
+    st.prepare()
+    st.data_dir = tmp_path
+    psi = launch_stage(st)
+    assert sorted(f.name for f in tmp_path.glob("psi_*.npy")) == ["psi_00000004.npy", "psi_00000006.npy"]
+    st2 = make(dict(type="load", path=str(tmp_path / "psi_00000006.npy")))
+    st2.prepare()
+    assert st2.psi.dtype == torch.complex64 and torch.equal(st2.psi, psi)
