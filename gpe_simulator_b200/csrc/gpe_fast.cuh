@@ -368,36 +368,6 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
   }
   small = __all_sync(0xffffffffu, small);
   tiny = __all_sync(0xffffffffu, tiny);
-  if (sizeof(R) == 4 && ph.local_fp64) {
-    // complex64 with the local factor evaluated and applied in FP64 (the phase
-    // recomputed from the same V and |psi|^2 in double)
-#pragma unroll
-    for (int s = 0; s < SLOTS; ++s) {
-      if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
-      int l, lane;
-      slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
-      const double c = (double)ctab[l];
-#pragma unroll
-      for (int a = 0; a < VALS; ++a) {
-        const int e = s * VALS + a, m = lane + LANES * a;
-        const double vz = (double)tb.vz[m];
-        double V = TWO ? 2.0 * vz + c : vz + c;
-        if (ARR) V += ph.vre ? (double)((const R*)ph.vre)[tl.base + (long long)l * tl.lstride + m] : 0.0;
-        const double vx = v[e].x, vy = v[e].y, hd = ph.dt * 0.5;
-        const double phd = (V + (TWO ? 2.0 : 1.0) * ph.beta * (vx * vx + vy * vy)) * hd;
-        if (!REAL) {
-          const double f = exp(-phd);
-          v[e] = mk((R)(vx * f), (R)(vy * f));
-        } else {
-          double sd, cd;
-          sincos(phd, &sd, &cd);
-          if (ARR) { const double am = exp((double)gam[e]); sd *= am; cd *= am; }
-          v[e] = mk((R)(vx * cd + vy * sd), (R)(vy * cd - vx * sd));
-        }
-      }
-    }
-    return;
-  }
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) {
     if (!slot_ok<N, R, LANES, SLOTS>(s)) break;

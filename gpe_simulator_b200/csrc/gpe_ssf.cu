@@ -538,9 +538,12 @@ int fill_plan(gpe_plan* p, const gpe_desc* d) {
     if (p->pp.radix[q] > 5 && p->pp.radix[q] != 8 && p->pp.radix[q] != 16) p->gen = true;
   p->ept = p->gen ? 8 : 16;
   // register-resident sweeps: n = 32, 48, 64, 96, 128, 160, 256; potentials from tables (no per-point program)
+  // (complex64 plans that evaluate the local factor in FP64 use the generic sweeps,
+  // which carry that variant; keeping it out of the register-resident kernels keeps
+  // their register budget)
   p->fast = (n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 160 || n == 256 ||
              (n == 512 && d->dtype == GPE_C64)) &&
-            d->generic_only != 1 && d->dynamic_g_len == 0;
+            d->generic_only != 1 && d->dynamic_g_len == 0 && !(d->local_fp64 && d->dtype == GPE_C64);
   p->plane = p->fast && d->dtype == GPE_C64 && (n == 128 || n == 256) && d->generic_only == 3;
   const int emax = 512 * p->ept;
   p->lt_yx = std::max(1, std::min(d->dtype == GPE_C64 ? 16 : 8, emax / n));
