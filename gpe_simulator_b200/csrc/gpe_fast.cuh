@@ -66,7 +66,17 @@ struct FastOps {
   int invm;         // FM_PLAIN: multiply by 1/M
   int scale;        // FM_Z1: apply the pending renormalisation
   int norm;         // FM_Z2: norm partials and renormalisation scale
+  int pdl;          // host: launch as a programmatic dependent of the previous sweep
 };
+
+// Programmatic dependent launch: a sweep lets the next one start (its blocks
+// then build their shared-memory tables while this sweep's last wave runs) and
+// waits for the previous sweep's results before touching psi.  Without a
+// programmatic launch the wait returns at once.
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // per-tile table bytes (kx, kyz, kx2, kyz2, vz, c1, c2, c12), rounded to 16
 template <int N, typename R> __host__ __device__ constexpr size_t fast_tables_bytes() {
@@ -539,6 +549,7 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   constexpr int S2 = FastCfg<N, R>::Q2;   // slots in layout (N2 lanes, N1 values)
   constexpr bool ZM = MODE == FM_Z1 || MODE == FM_Z2 || MODE == FM_Z21;
   using TW = typename TwE<R>::T;
+  griddep_launch_dependents();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* ex = (C*)smem_raw + 2 * N;   // after the twiddle table (N entries of 16 bytes)
   Acc* red = (Acc*)(ex + fast_exchange_elems<N, R>());
@@ -575,6 +586,9 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   const FastTile<N, AX, R> tl(tile);
   if (ZM) z_tables<N, R>(ph, sw, tl.a0, tb, MODE == FM_Z21);
   if (MODE == FM_XKIN) x_tables<N, R>(ph, tl.a0, tl.b0, tb);
+  // everything above reads plan constants only; psi and the renormalisation scale
+  // come from the previous sweep
+  griddep_wait();
   PwCtx<R> cx;
   cx.sc_div = 1.0;
   cx.sc_mul = (R)1;

@@ -32,8 +32,21 @@ static cudaError_t launch_fast_one(const Phys& ph, const Sweep& sw, const FastOp
     if (e != cudaSuccess) return e;
     attr_dev = dev;
   }
-  kern<<<tiles, T, smem, st>>>(ph, sw, op);
-  return cudaGetLastError();
+  if (!op.pdl) {
+    kern<<<tiles, T, smem, st>>>(ph, sw, op);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)tiles);
+  cfg.blockDim = dim3(T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, ph, sw, op);
 }
 
 template <int N, typename R>

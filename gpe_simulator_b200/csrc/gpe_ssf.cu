@@ -286,6 +286,8 @@ struct gpe_plan {
   bool gen = false;                // grid size needs the odd-prime radices 7/11/13
   bool fast = false;               // register-resident sweeps exist for this n
   bool plane = false;              // y and z sweeps fused per x-plane (opt-in; complex64, n = 128, 256)
+  bool pdl_chain = false;          // inside a step sequence: sweeps may launch programmatically
+  bool pdl_prev = false;           // a sweep of the current sequence has been launched
   int ept = 16;                    // elements per thread of the sweep family
   int nbins = 0;
   double shell_w = 0;
@@ -407,8 +409,11 @@ int fsweep(gpe_plan* p, int ax, Sweep sw, const FastOps& op, cudaStream_t st) {
     CU(cudaEventRecord(r.a, st));
   }
   const int fax = ax == AX_Z ? FZ : ax == AX_Y ? FY : FX;
-  const cudaError_t e = p->dtype == GPE_C64 ? launch_fast<float>(p->n, fax, p->ph, sw, op, st)
-                                            : launch_fast<double>(p->n, fax, p->ph, sw, op, st);
+  FastOps o = op;
+  o.pdl = p->pdl_chain && p->pdl_prev && !p->prof ? 1 : 0;
+  p->pdl_prev = p->pdl_chain;
+  const cudaError_t e = p->dtype == GPE_C64 ? launch_fast<float>(p->n, fax, p->ph, sw, o, st)
+                                            : launch_fast<double>(p->n, fax, p->ph, sw, o, st);
   if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("fast sweep: ") + cudaGetErrorString(e));
   ++p->launches;
   if (p->prof) {
@@ -448,6 +453,7 @@ int psweep(gpe_plan* p, void* psi, int mz, const FastOps* ops, int nstage, int z
     r.b = pooled_event(p);
     CU(cudaEventRecord(r.a, st));
   }
+  p->pdl_prev = false;   // the sweep after a persistent plane launch starts normally
   const cudaError_t e = launch_plane<float>(p->n, mz, p->ph, sw, job, st);
   if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("plane sweep: ") + cudaGetErrorString(e));
   ++p->launches;
@@ -460,9 +466,18 @@ int psweep(gpe_plan* p, void* psi, int mz, const FastOps* ops, int nstage, int z
 
 FastOps mk_ops(int mode, int inv1 = 0, int invm = 0, int scale = 0, int norm = 0) {
   FastOps o;
-  o.mode = mode; o.inv1 = inv1; o.invm = invm; o.scale = scale; o.norm = norm;
+  o.mode = mode; o.inv1 = inv1; o.invm = invm; o.scale = scale; o.norm = norm; o.pdl = 0;
   return o;
 }
+
+// Scope of one step sequence: its register-resident sweeps after the first are
+// launched as programmatic dependents of the sweep before (they read only plan
+// constants until their grid-dependency wait).
+struct PdlChain {
+  gpe_plan* p;
+  explicit PdlChain(gpe_plan* q) : p(q) { p->pdl_chain = true; p->pdl_prev = false; }
+  ~PdlChain() { p->pdl_chain = false; p->pdl_prev = false; }
+};
 
 Sweep mk_sweep(const void* src, void* dst) {
   Sweep s;
@@ -997,6 +1012,7 @@ int gpe_step(gpe_plan* p, void* psi, int nsteps, long long step0, void* stream) 
   if (nsteps < 0) return fail(GPE_ERR_ARG, "nsteps must be >= 0");
   cudaStream_t st = (cudaStream_t)stream;
   const bool imag = p->kind == GPE_IMAGINARY;
+  PdlChain chain(p);
   if (p->plane && nsteps > 0) {
     // per step: XKIN, then one plane-fused launch [inverse y, z, forward y]; the
     // first call opens with [Z1, forward y], the last step ends with [inverse y, Z2]
@@ -1048,6 +1064,7 @@ int gpe_step_at(gpe_plan* p, void* psi, double t, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   // reference: t_mid = float(t) + dt/2 (gpe/make_propagator.py:94)
   const double tm = t + p->dt / 2;
+  PdlChain chain(p);
   if (p->fast) {
     TRY(fast_front(p, psi, tm, false, st));
     TRY(fast_middle(p, psi, st));
