@@ -262,14 +262,11 @@ __device__ __forceinline__ void z_tables(const Phys& ph, const Sweep& sw, int a0
     const R base = vax[i] + vax[N + j];
     R b1 = (R)0, b2 = (R)0;
     if (ph.kind == 1 && ph.beam) {
-      // separable beam: amp * exp(-(x-cx)^2/w^2) * exp(-(y-cy)^2/w^2), centre from an FP64 angle
-      double cx, cy;
-      beam_centre(ph, sw.t1, cx, cy);
-      const R dx = (R)(ph.x[i] - cx), dy = (R)(ph.x[j] - cy), iw = (R)ph.beam_inv_w2;
+      // separable beam: amp * exp(-(x-cx)^2/w^2) * exp(-(y-cy)^2/w^2); centres from the host
+      const R dx = (R)(ph.x[i] - sw.bc1x), dy = (R)(ph.x[j] - sw.bc1y), iw = (R)ph.beam_inv_w2;
       b1 = (R)ph.beam_amp * rexp(-dx * dx * iw) * rexp(-dy * dy * iw);
       if (two) {
-        beam_centre(ph, sw.t2, cx, cy);
-        const R ex = (R)(ph.x[i] - cx), ey = (R)(ph.x[j] - cy);
+        const R ex = (R)(ph.x[i] - sw.bc2x), ey = (R)(ph.x[j] - sw.bc2y);
         b2 = (R)ph.beam_amp * rexp(-ex * ex * iw) * rexp(-ey * ey * iw);
       }
     }

@@ -57,6 +57,8 @@ struct Sweep {
   unsigned pre, mid, post;
   int fft1, fft2;        // run FFT #1 / #2
   double t1, t2;         // times of the half-steps PW_HALF1 / PW_HALF2 (t_mid of the step)
+  double bc1x, bc1y;     // stirring-beam centre at t1 and t2 (FP64 angle, set by the host
+  double bc2x, bc2y;     //   once per launch)
   double* partial;       // per-block partial sums (PW_NORM: 1 double; diag: several)
   unsigned* ticket;      // last-block ticket
   double* scale;         // [0] = sqrt(N) of the last renormalisation, [1] = 1/sqrt(N)
@@ -157,20 +159,6 @@ static __device__ double eval_program(const double* prog, int len, double x, dou
 }
 
 // Beam centre for a time; angle accumulated in FP64.
-__device__ __forceinline__ void beam_centre(const Phys& ph, double t, double& cx, double& cy) {
-  double th;
-  if (ph.beam_t_ramp > 0.0) {
-    const double m = fmin(t, ph.beam_t_ramp);
-    th = ph.beam_omega * (m * m / (2.0 * ph.beam_t_ramp) + t - m);
-  } else {
-    th = ph.beam_omega * t;
-  }
-  double s, c;
-  sincos(th, &s, &c);
-  cx = ph.beam_radius * c;
-  cy = ph.beam_radius * s;
-}
-
 __device__ __forceinline__ void rsincos(float a, float* s, float* c) { sincosf(a, s, c); }
 __device__ __forceinline__ void rsincos(double a, double* s, double* c) { sincos(a, s, c); }
 __device__ __forceinline__ float rexp(float a) { return expf(a); }
@@ -371,11 +359,10 @@ template <typename R>
 __device__ void setup_ctx(const Phys& ph, const Sweep& sw, unsigned all_ops, PwCtx<R>& cx) {
   cx.t1 = sw.t1;
   cx.t2 = sw.t2;
-  cx.b1x = cx.b1y = cx.b2x = cx.b2y = 0.0;
-  if (ph.kind == 1 && ph.beam) {
-    beam_centre(ph, cx.t1, cx.b1x, cx.b1y);
-    beam_centre(ph, cx.t2, cx.b2x, cx.b2y);
-  }
+  cx.b1x = sw.bc1x;
+  cx.b1y = sw.bc1y;
+  cx.b2x = sw.bc2x;
+  cx.b2y = sw.bc2y;
   cx.sc_div = 1.0;
   cx.sc_mul = (R)1;
   if (all_ops & PW_SCALE) {

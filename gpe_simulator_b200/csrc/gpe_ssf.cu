@@ -378,7 +378,31 @@ cudaEvent_t pooled_event(gpe_plan* p) {
   return e;
 }
 
-int sweep(gpe_plan* p, int ax, const Sweep& sw, cudaStream_t st) {
+// Centres of the stirring beam at the sweep's half-step times t1, t2: the angle
+// th(t) = omega (m^2/(2 t_ramp) + t - m), m = min(t, t_ramp) (linear ramp of the
+// angular rate), in FP64 once per launch.
+void beam_centres(const gpe_plan* p, Sweep& sw) {
+  sw.bc1x = sw.bc1y = sw.bc2x = sw.bc2y = 0.0;
+  if (!(p->kind == GPE_REAL && p->ph.beam)) return;
+  const Phys& ph = p->ph;
+  auto centre = [&](double t, double& cx, double& cy) {
+    double th;
+    if (ph.beam_t_ramp > 0.0) {
+      const double m = std::min(t, ph.beam_t_ramp);
+      th = ph.beam_omega * (m * m / (2.0 * ph.beam_t_ramp) + t - m);
+    } else {
+      th = ph.beam_omega * t;
+    }
+    cx = ph.beam_radius * std::cos(th);
+    cy = ph.beam_radius * std::sin(th);
+  };
+  centre(sw.t1, sw.bc1x, sw.bc1y);
+  centre(sw.t2, sw.bc2x, sw.bc2y);
+}
+
+int sweep(gpe_plan* p, int ax, const Sweep& sw_in, cudaStream_t st) {
+  Sweep sw = sw_in;
+  beam_centres(p, sw);
   gpe_plan::Rec r{ax, nullptr, nullptr};
   if (p->prof) {
     r.a = pooled_event(p);
@@ -396,6 +420,7 @@ int sweep(gpe_plan* p, int ax, const Sweep& sw, cudaStream_t st) {
 
 // Register-resident sweep (n in {64, 128, 256}); same accounting as sweep().
 int fsweep(gpe_plan* p, int ax, Sweep sw, const FastOps& op, cudaStream_t st) {
+  beam_centres(p, sw);
   sw.pp = p->pp;
   sw.tw = p->d_tw;
   sw.tw_lo = (const char*)p->d_tw + (size_t)p->n * p->csize;
@@ -434,6 +459,7 @@ int psweep(gpe_plan* p, void* psi, int mz, const FastOps* ops, int nstage, int z
   sw.dst = psi;
   sw.t1 = t1;
   sw.t2 = t2;
+  beam_centres(p, sw);
   sw.partial = p->d_partial;
   sw.pp = p->pp;
   sw.tw = p->d_tw;
