@@ -564,7 +564,9 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   // complex64 entries pack hi and lo
   TW* t1 = (TW*)smem_raw;
   TW* t2 = (N1 == N2) ? t1 : (TW*)(tail + fast_tables_bytes<N, R>());
-  {
+  const FastTile<N, AX, R> tl(tile);
+  // shared-memory tables: plan constants only (twiddles, potential and kinetic tables)
+  auto prologue = [&]() {
     const C* gh = (const C*)sw.tw;
     const C* gl = (const C*)sw.tw_lo;
     auto entry = [&](int e) -> TW {
@@ -579,12 +581,13 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
         t2[q] = entry(n2 * k2b);
       }
     }
-  }
-  const FastTile<N, AX, R> tl(tile);
-  if (ZM) z_tables<N, R>(ph, sw, tl.a0, tb, MODE == FM_Z21);
-  if (MODE == FM_XKIN) x_tables<N, R>(ph, tl.a0, tl.b0, tb);
-  // everything above reads plan constants only; psi and the renormalisation scale
-  // come from the previous sweep
+    if (ZM) z_tables<N, R>(ph, sw, tl.a0, tb, MODE == FM_Z21);
+    if (MODE == FM_XKIN) x_tables<N, R>(ph, tl.a0, tl.b0, tb);
+  };
+  // psi and the renormalisation scale come from the previous sweep: read them
+  // after the grid-dependency wait; the tile's loads are issued first and are in
+  // flight while the tables are built (measured faster than building the tables
+  // before the wait, where only the first wave would overlap them)
   griddep_wait();
   PwCtx<R> cx;
   cx.sc_div = 1.0;
@@ -596,6 +599,7 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
 
   C v[EPT];
   fast_load<N, AX, R, S1, CG>(v, tl, (const C*)sw.src, MODE == FM_Z2 || MODE == FM_Z21 || (MODE == FM_PLAIN && op.inv1));
+  prologue();
   __syncthreads();  // twiddles and tables visible
   if (MODE == FM_Z1) fast_pointwise<N, AX, R, MODE, 0, N1, N2, S1>(v, tl, ph, tb, op, cx);
   fft_2phase<N, N1, N2, AX, R, S1, S2, EPT>(v, ex, t1);
