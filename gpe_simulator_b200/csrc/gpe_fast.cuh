@@ -627,9 +627,13 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
 // compiler's choice.  Measured for complex64 at n = 128, 256: the plain FFT
 // sweeps are memory-bound and want 1024 threads per SM (64 registers at
 // T = 256); the fused modes keep 768 (85 registers) for their extra live state.
+// At n = 512 (32-point phase, up to 214 registers unbounded) 768 / 512 threads
+// per SM: 240 -> 291 steps/s at 512^3 despite a few hundred bytes of spills.
 template <int N, typename R, int MODE> struct FastBounds {
   static constexpr int value = (sizeof(R) == 4 && (N == 128 || N == 256))
-                                   ? (MODE == FM_PLAIN ? 1024 : 768) / FastCfg<N, R>::T : 0;
+                                   ? (MODE == FM_PLAIN ? 1024 : 768) / FastCfg<N, R>::T
+                               : (sizeof(R) == 4 && N == 512)
+                                   ? (MODE == FM_PLAIN ? 768 : 512) / FastCfg<N, R>::T : 0;
 };
 
 template <int N, int AX, typename R, int MODE>
