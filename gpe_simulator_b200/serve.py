@@ -117,11 +117,14 @@ class Server:
     """Continuous batching over a running imaginary-time :class:`Batch` and
     real-time segments on per-session streams (see the module docstring)."""
 
-    def __init__(self, sessions, dtype=torch.complex64, budget=150e9, chunk=20):
+    def __init__(self, sessions, dtype=torch.complex64, budget=150e9, chunk=20, max_active=None):
         self.sessions = sessions
         self.dtype = dtype
         self.budget = budget
         self.chunk = chunk
+        # at most this many imaginary-time solves advance together (None: as many as
+        # the memory budget admits); fewer finish sooner, more share each launch
+        self.max_active = max_active
         self.streams = [torch.cuda.Stream() for _ in sessions]
         self.batch_stream = torch.cuda.Stream()
 
@@ -146,7 +149,8 @@ class Server:
             for r in queue:
                 if r.kind == "imaginary":
                     need = state_bytes(r.inst.n, self.dtype)
-                    if used + need > self.budget:
+                    full = self.max_active is not None and len(imag) >= self.max_active
+                    if used + need > self.budget or full:
                         keep.append(r)
                         continue
                     with torch.cuda.stream(self.batch_stream):
