@@ -38,6 +38,7 @@ class Desc(ctypes.Structure):
         ("nk_bins", ctypes.c_int),
         ("local_fp64", ctypes.c_int),
         ("generic_only", ctypes.c_int),
+        ("exact_local", ctypes.c_int),
     ]
 
 

@@ -44,6 +44,7 @@ struct Phys {
   int kcut;
   double kcut2;
   int local_fp64;        // complex64: evaluate the local half-step factor in FP64
+  int exact_local;       // exact local sub-flows (FP64), not the reference's frozen density
 };
 
 struct Sweep {
@@ -187,6 +188,25 @@ __device__ __forceinline__ typename Cx<R>::T halfstep(const Phys& ph, typename C
                                                       int j, int k, long long idx, double t, double bcx,
                                                       double bcy) {
   const R V = potential<R>(ph, n, i, j, k, idx, t, bcx, bcy);
+  if (ph.exact_local) {
+    // exact flows of the local subproblem over h = dt/2 (V held fixed):
+    //   imaginary  d psi/dt = -(V + beta|psi|^2) psi:
+    //              psi e^{-Vh} / sqrt(1 + 2 beta |psi|^2 s), s = (1 - e^{-2Vh}) / (2V)
+    //   real       i d psi/dt = (V - i Gamma + beta|psi|^2) psi: |psi|^2 decays as e^{-2 Gamma t},
+    //              phase V h + beta |psi|^2 tau, tau = (1 - e^{-2 Gamma h}) / (2 Gamma)
+    const double vx = v.x, vy = v.y, h = ph.dt * 0.5, rho = vx * vx + vy * vy, Vd = (double)V;
+    if (ph.kind == 0) {
+      const double s = Vd == 0.0 ? h : -expm1(-2.0 * Vd * h) / (2.0 * Vd);
+      const double f = exp(-Vd * h) / sqrt(1.0 + 2.0 * ph.beta * rho * s);
+      return mk((R)(vx * f), (R)(vy * f));
+    }
+    const double g = ph.vim ? -(double)((const R*)ph.vim)[idx] : 0.0;   // Gamma
+    const double tau = g == 0.0 ? h : -expm1(-2.0 * g * h) / (2.0 * g);
+    double sd, cd;
+    sincos(Vd * h + ph.beta * rho * tau, &sd, &cd);
+    const double a = exp(-g * h);
+    return mk((R)((vx * cd + vy * sd) * a), (R)((vy * cd - vx * sd) * a));
+  }
   if (sizeof(R) == 4 && ph.local_fp64) {
     // complex64 data, local factor evaluated and applied in FP64
     const double vx = v.x, vy = v.y, hd = ph.dt * 0.5;

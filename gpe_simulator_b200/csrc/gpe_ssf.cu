@@ -584,7 +584,8 @@ int fill_plan(gpe_plan* p, const gpe_desc* d) {
   // their register budget)
   p->fast = (n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 160 || n == 256 ||
              (n == 512 && d->dtype == GPE_C64)) &&
-            d->generic_only != 1 && d->dynamic_g_len == 0 && !(d->local_fp64 && d->dtype == GPE_C64);
+            d->generic_only != 1 && d->dynamic_g_len == 0 && !(d->local_fp64 && d->dtype == GPE_C64) &&
+            !d->exact_local;
   p->plane = p->fast && d->dtype == GPE_C64 && (n == 128 || n == 256) && d->generic_only == 3;
   const int emax = 512 * p->ept;
   p->lt_yx = std::max(1, std::min(d->dtype == GPE_C64 ? 16 : 8, emax / n));
@@ -748,6 +749,7 @@ int create(const gpe_desc* d, gpe_plan** out) {
   ph.kcut = d->k_cut_enabled ? 1 : 0;
   ph.kcut2 = d->k_cut * d->k_cut;
   ph.local_fp64 = d->local_fp64 ? 1 : 0;
+  ph.exact_local = d->exact_local ? 1 : 0;
   rc = build_static(p, nullptr, GPE_V_NONE, 0);
   if (rc != GPE_OK) { free_plan(p); return rc; }
   CU(cudaDeviceSynchronize());

@@ -48,7 +48,7 @@ def _dptr(values):
 class Plan:
     def __init__(self, n, x_array, k_array, *, dtype, kind, beta, dt, kinetic_coeff=1.0,
                  static_expr="0", dynamic_expr="0", k_cut=None, beam=None, nk_bins=0,
-                 local_fp64=None, generic_only=False, fuse_planes=False):
+                 local_fp64=None, generic_only=False, fuse_planes=False, exact_local=False):
         if not torch.cuda.is_available():
             raise RuntimeError("gpe_simulator_b200 needs a CUDA device (sm_100a)")
         self.lib = _lib.load()
@@ -101,6 +101,8 @@ class Plan:
         d.local_fp64 = 1 if local_fp64 else 0
         # sweep path: 0 fastest, 1 generic only, 3 y/z sweeps fused per x-plane (complex64 n = 128, 256)
         d.generic_only = 1 if generic_only else (3 if fuse_planes else 0)
+        # exact local sub-flows: an accuracy mode that departs from the reference on purpose
+        d.exact_local = 1 if exact_local else 0
         self.local_fp64 = bool(local_fp64)
         handle = ctypes.c_void_p()
         with torch.cuda.device(self.device):

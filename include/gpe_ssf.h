@@ -124,6 +124,13 @@ typedef struct gpe_desc {
      * instead of once per sweep; identical results, measured slower on B200
      * because the sweeps are issue-bound, not HBM-bound). */
     int generic_only;
+    /* 1 = exact local sub-flows (an accuracy mode that departs from the reference
+     * on purpose; evaluated in FP64 on the generic sweeps): imaginary time
+     * psi e^{-Vh} / sqrt(1 + 2 beta |psi|^2 s), s = -expm1(-2Vh)/(2V) (h at V = 0);
+     * real time with an absorber U - i Gamma, nonlinear phase beta |psi|^2 tau,
+     * tau = -expm1(-2 Gamma h)/(2 Gamma) (h at Gamma = 0).  0 = the reference's
+     * frozen-density half-step. */
+    int exact_local;
 } gpe_desc;
 
 /* library */

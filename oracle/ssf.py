@@ -142,6 +142,7 @@ class Model:
     static_v: np.ndarray = None   # real (imag time) or complex U - i Gamma (real time)
     k_cut: float = None
     beam: Beam = None
+    exact_local: bool = False     # exact local sub-flows (not the reference's; parity off)
     x: np.ndarray = field(init=False)
     k: np.ndarray = field(init=False)
 
@@ -192,6 +193,20 @@ def halfstep(psi, model, t_mid=0.0):
     h = model.dt / 2
     rdt = np.float64 if psi.dtype == np.complex128 else np.float32
     abs2 = psi.real.astype(np.float64) ** 2 + psi.imag.astype(np.float64) ** 2
+    if model.exact_local:
+        # exact flows of the local subproblem with V fixed over h (the reference's
+        # notes, "GPE simulator/HANDOFF.md" accepted approximations): imaginary time
+        # psi e^{-Vh}/sqrt(1 + 2 beta|psi|^2 s); real time with Gamma = -Im V,
+        # phase Vh + beta|psi|^2 tau and amplitude e^{-Gamma h}
+        with np.errstate(divide="ignore", invalid="ignore"):
+            if model.kind == "imaginary":
+                s = np.where(v == 0, h, -np.expm1(-2 * v * h) / (2 * v))
+                psi *= (np.exp(-v * h) / np.sqrt(1 + 2 * model.beta * abs2 * s)).astype(rdt)
+            else:
+                g = -np.broadcast_to(model.loss(), v.shape)
+                tau = np.where(g == 0, h, -np.expm1(-2 * g * h) / (2 * g))
+                psi *= np.exp(-g * h - 1j * (v * h + model.beta * abs2 * tau)).astype(psi.dtype)
+        return psi
     phase = (v + model.beta * abs2) * h
     if model.kind == "imaginary":
         psi *= np.exp(-phase).astype(rdt)

@@ -198,3 +198,34 @@ def test_closure_takes_dlpack_arrays_in_place(cuda, kind):
         assert out is b.psi
     torch.cuda.synchronize()
     assert torch.equal(a.psi, raw)
+
+
+@pytest.mark.parametrize("kind", ["imaginary", "real"])
+@pytest.mark.parametrize("dtype,tol", [(torch.complex128, 1e-12), (torch.complex64, 2e-5)])
+def test_exact_local_mode_matches_oracle(cuda, kind, dtype, tol):
+    """The opt-in exact local sub-flows (imaginary time; real time with an
+    absorber) against the oracle's restatement; the default stays the reference's."""
+    from gpe_simulator_b200 import Plan
+    from oracle import ssf
+    from tests.golden import cases
+    c = cases.LOSSY16
+    n, L, expr = 16, 8.0, "0.5*x**2+0.5*y**2+z**2/4"
+    x, k = ssf.get_grids(n, L)
+    static_v = cases.lossy_potential(x, c) if kind == "real" else None
+    kw = dict(dtype=dtype, kind=kind, beta=300.0, dt=2e-3, static_expr=expr)
+    exact, plain = Plan(n, x, k, exact_local=True, **kw), Plan(n, x, k, **kw)
+    if static_v is not None:
+        for p in (exact, plain):
+            p.set_static_potential(torch.from_numpy(static_v).cuda())
+    psi0 = ssf.noisy_gaussian(x, seed=2)
+    a = torch.from_numpy(psi0).to(dtype).cuda()
+    b = a.clone()
+    exact.step(a, 20, 0)
+    plain.step(b, 20, 0)
+    m = ssf.Model(n=n, simulation_range=L, kind=kind, beta=300.0, dt=2e-3, static_expr=expr,
+                  static_v=static_v, exact_local=True)
+    want = ssf.run(psi0, m, 20)
+    assert ssf.rel_l2(a.cpu().numpy().astype(np.complex128), want) < tol
+    # the default is the reference's frozen-density step (the two differ at second
+    # order in beta |psi|^2 dt/2, so only a little at this step size)
+    assert not torch.equal(a, b)

@@ -195,3 +195,42 @@ def test_projections_against_reference_save_outputs(n, L):
     for key in ssf.PROJECTIONS:
         np.testing.assert_array_equal(np.isnan(out[key]), np.isnan(g[key]))
         np.testing.assert_allclose(np.nan_to_num(out[key]), np.nan_to_num(g[key]), rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("kind", ["imaginary", "real"])
+def test_exact_local_flow_is_the_limit_of_frozen_density_substeps(kind):
+    """The exact local sub-flow (an opt-in accuracy mode) equals the limit of
+    many frozen-density micro-steps of the same local equation, with the trap
+    and, in real time, an absorber U - i Gamma."""
+    n, L = 8, 8.0
+    x, _ = ssf.get_grids(n, L)
+    X, Y, Z = x[:, None, None], x[None, :, None], x[None, None, :]
+    static_v = None
+    if kind == "real":
+        static_v = (0.3 * X ** 2 - 1j * (0.8 + 0.5 * np.tanh(Y))).astype(np.complex128) * np.ones((n, n, n))
+    kw = dict(n=n, simulation_range=L, kind=kind, beta=900.0, dt=0.02, static_expr="x**2+2*y**2+0.5*z**2",
+              static_v=static_v)
+    psi0 = ssf.noisy_gaussian(x, seed=2)
+    exact = ssf.halfstep(psi0.copy(), ssf.Model(exact_local=True, **kw))
+    micro = ssf.Model(**{**kw, "dt": kw["dt"] / 4000})
+    fine = psi0.copy()
+    for _ in range(4000):
+        ssf.halfstep(fine, micro)
+    assert ssf.rel_l2(exact, fine) < 2e-4          # first order in the micro step
+    plain = ssf.halfstep(psi0.copy(), ssf.Model(**kw))
+    assert ssf.rel_l2(exact, fine) < 0.05 * ssf.rel_l2(plain, fine)
+
+
+def test_exact_local_closed_forms_for_uniform_states():
+    n, L, beta, dt = 4, 4.0, 50.0, 0.1
+    h = dt / 2
+    c = 0.3 + 0.2j
+    rho = abs(c) ** 2
+    psi = np.full((n, n, n), c)
+    m = ssf.Model(n=n, simulation_range=L, kind="imaginary", beta=beta, dt=dt, exact_local=True)
+    np.testing.assert_allclose(ssf.halfstep(psi.copy(), m), c / np.sqrt(1 + 2 * beta * rho * h), rtol=1e-14)
+    g = 0.7
+    m = ssf.Model(n=n, simulation_range=L, kind="real", beta=beta, dt=dt, exact_local=True,
+                  static_v=np.full((n, n, n), -1j * g))
+    tau = -np.expm1(-2 * g * h) / (2 * g)
+    np.testing.assert_allclose(ssf.halfstep(psi.copy(), m), c * np.exp(-g * h - 1j * beta * rho * tau), rtol=1e-14)
