@@ -2,8 +2,8 @@
 
 The fixtures (``tests/golden/*.npz``, made by ``tests/golden/make_golden.py``)
 hold the reference's own outputs (its propagator closures, kernel strings and
-diagnostics, with numpy.fft in place of cuFFT).  complex128 must match to the
-north-star tolerance 1e-12 (psi relative L2); complex64 to 1e-5.
+diagnostics, with numpy.fft in place of cuFFT).  complex128 must match to
+1e-12 (psi relative L2); complex64 to 1e-5.
 """
 
 from pathlib import Path

@@ -2,7 +2,6 @@
 precisions, the reference's checks, and files exchanged with the reference's own
 save/load (run on the host through the oracle shim, where the reference exists)."""
 
-from pathlib import Path
 from types import SimpleNamespace
 
 import numpy as np
@@ -11,7 +10,7 @@ import torch
 
 from gpe_simulator_b200.state_io import load_wavefunction, save_wavefunction
 
-REFERENCE = Path("/root/reference")
+from oracle.ref_shim import REFERENCE  # noqa: E402
 
 
 def make_stage(n=8, L=6.0, dtype=torch.complex64, seed=0):
