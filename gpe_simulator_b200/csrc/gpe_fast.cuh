@@ -479,14 +479,18 @@ __device__ __forceinline__ void fast_pointwise(typename Cx<R>::T (&v)[EPT], cons
   half_dispatch<N, AX, R, LANES, VALS, SLOTS, EPT>(v, tl, ph, tb, tb.c1);
   if (MODE == FM_Z21) half_dispatch<N, AX, R, LANES, VALS, SLOTS, EPT>(v, tl, ph, tb, tb.c2);
   if (MODE == FM_Z2 && op.norm) {
+    // a thread's few values summed in plain FP64 (fixed order), the thread sums
+    // then combined with compensation across the block and the grid
 #pragma unroll
     for (int s = 0; s < SLOTS; ++s) {
       if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
+      double sum = 0.0;
 #pragma unroll
       for (int a = 0; a < VALS; ++a) {
         const typename Cx<R>::T x = v[s * VALS + a];
-        cx.acc[0].add((double)x.x * x.x + (double)x.y * x.y);
+        sum = fma((double)x.x, (double)x.x, fma((double)x.y, (double)x.y, sum));
       }
+      cx.acc[0].add(sum);
     }
   }
 }
