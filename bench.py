@@ -479,7 +479,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 512^3 leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
-    ap.add_argument("--serve-requests", type=int, default=60)
+    ap.add_argument("--serve-requests", type=int, default=120)
     ap.add_argument("--serve-rate", type=float, default=50.0)
     args = ap.parse_args()
     if args.warmup < 3:
