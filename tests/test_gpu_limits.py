@@ -78,3 +78,28 @@ def test_stirred_256_is_time_reversible(cuda, dtype, tol, path):
     err = ((psi - psi0).abs().pow(2).sum() / psi0.abs().pow(2).sum()).sqrt().item()
     assert moved > 1e-2                          # the state did evolve
     assert err < tol, err
+
+
+def test_stirred_512_is_time_reversible(cuda):
+    """The 512^3 register-resident sweeps (complex64): 20 fused steps forward and
+    20 back with -dt return to the start."""
+    from gpe_simulator_b200 import Plan, beam_in_reference_units
+    n, L, dt = 512, 24.0, 1.25e-4
+    x = np.linspace(-L / 2, L / 2, n, endpoint=False)
+    k = 2 * np.pi * np.fft.fftfreq(n, L / n)
+    beam = beam_in_reference_units(10.0, 0.5, 2.0, 0.5, 200 * 2.5e-4)
+    kw = dict(dtype=torch.complex64, kind="real", beta=4000.0, static_expr="x**2+1.44*y**2+2.25*z**2",
+              beam=beam)
+    fwd, back = Plan(n, x, k, dt=dt, **kw), Plan(n, x, k, dt=-dt, **kw)
+    g = torch.from_numpy(np.exp(-x ** 2 / 2)).cuda()
+    psi0 = (g[:, None, None] * g[None, :, None] * g[None, None, :]).to(torch.complex64)
+    psi0 = psi0 * (1 + 0.01 * torch.randn(psi0.shape, dtype=torch.complex64, device="cuda",
+                                          generator=torch.Generator(device="cuda").manual_seed(3)))
+    fwd.normalise(psi0)
+    psi = psi0.clone()
+    fwd.step(psi, 20, 0)
+    moved = ((psi - psi0).abs().pow(2).sum() / psi0.abs().pow(2).sum()).sqrt().item()
+    back.step(psi, 20, -20)
+    err = ((psi - psi0).abs().pow(2).sum() / psi0.abs().pow(2).sum()).sqrt().item()
+    assert moved > 1e-3
+    assert err < 2e-5, err
