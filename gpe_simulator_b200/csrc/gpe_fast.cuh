@@ -78,6 +78,12 @@ __device__ __forceinline__ void griddep_launch_dependents() {
 }
 __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Order this thread's generic-proxy shared-memory accesses before later
+// async-proxy (TMA) accesses of the same bytes.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // per-tile table bytes (kx, kyz, kx2, kyz2, vz, c1, c2, c12), rounded to 16
 template <int N, typename R> __host__ __device__ constexpr size_t fast_tables_bytes() {
   return (((size_t)(N + FastCfg<N, R>::L) * (16 + 8) + (size_t)(N + 3 * FastCfg<N, R>::L) * sizeof(R)) + 15)
@@ -133,13 +139,15 @@ __device__ __forceinline__ void slot(int gs, int per, int& l, int& lane) {
 // One forward FFT of every line of the tile, A = lanes in phase 1 (values A-strided),
 // B = values per lane in phase 1.  In: v[s][b] = x[lane_s + A*b] of line l_s (phase-1
 // slots).  Out: v[s][a] = X[lane_s + B*a] (phase-2 slots with B lanes per line).
-template <int N, int A, int B, int AX, typename R, int QA, int QB, int V>
+template <int N, int A, int B, int AX, typename R, int QA, int QB, int V, bool ASYNC_NEXT = false>
 __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename Cx<R>::T* ex,
                                            const typename TwE<R>::T* tw) {
   // In: QA slots of (A lanes, B values), slot s holding x[lane + A*b] in v[s*B + b].
   // Out: QB slots of (B lanes, A values), slot s holding X[lane + B*a] in v[s*A + a].
   // tw: 2-D twiddle table of this split, tw[k2*A + lane] = W_N^(lane*k2) ({hi, lo}
   // for complex64): consecutive lanes read consecutive entries.
+  // ASYNC_NEXT: the exchange buffer is overwritten by a TMA copy after the final
+  // barrier, so each thread fences its exchange accesses against the async proxy.
   using C = typename Cx<R>::T;
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
@@ -181,6 +189,7 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
     }
     Dft<A>::run(x, (const C*)nullptr, (const C*)nullptr, N / A);
   }
+  if (ASYNC_NEXT) fence_proxy_async_smem();
   if (WARP_LOCAL) __syncwarp(); else __syncthreads();
 }
 

@@ -1,5 +1,6 @@
 // Dispatch of the register-resident sweeps by grid size (one translation unit per
 // size and precision holds the kernels: gpe_fast_<prec>_<n>.cu).
+#include <cuda.h>
 #include "gpe_fast.cuh"
 
 namespace gpe {
@@ -38,6 +39,20 @@ cudaError_t launch_fast_batch(int n, int ax, const Phys* phs, const Sweep* sws, 
     case 512:
       if constexpr (sizeof(R) == 4) return launch_fastb_n<512, float>(ax, phs, sws, count, op, st);
       return cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int N>
+cudaError_t launch_tma_n(int ax, const Phys& ph, const Sweep& sw, const FastOps& op, const CUtensorMap& map,
+                         cudaStream_t st);
+
+// TMA-staged plain y/x sweeps: complex64, n = 128 and 256
+cudaError_t launch_fast_tma(int n, int ax, const Phys& ph, const Sweep& sw, const FastOps& op,
+                            const CUtensorMap& map, cudaStream_t st) {
+  switch (n) {
+    case 128: return launch_tma_n<128>(ax, ph, sw, op, map, st);
+    case 256: return launch_tma_n<256>(ax, ph, sw, op, map, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -6,3 +6,5 @@ template cudaError_t gpe::launch_fastb_n<256, float>(int, const gpe::Phys*, cons
                                                   const gpe::FastOps&, cudaStream_t);
 template cudaError_t gpe::launch_plane_n<256, float>(int, const gpe::Phys&, const gpe::Sweep&, gpe::PlaneJob,
                                                      cudaStream_t);
+template cudaError_t gpe::launch_tma_n<256>(int, const gpe::Phys&, const gpe::Sweep&, const gpe::FastOps&,
+                                          const CUtensorMap&, cudaStream_t);

@@ -2,6 +2,7 @@
 #pragma once
 #include "gpe_fast.cuh"
 #include "gpe_sweep.h"
+#include "gpe_tma.cuh"
 
 namespace gpe {
 
@@ -96,6 +97,57 @@ cudaError_t launch_fastb_n(int ax, const Phys* phs, const Sweep* sws, int count,
   if (ax == FZ) return launch_fastb_one<N, FZ, R, FM_PLAIN>(phs, sws, count, op, st);
   if (ax == FY) return launch_fastb_one<N, FY, R, FM_PLAIN>(phs, sws, count, op, st);
   return launch_fastb_one<N, FX, R, FM_PLAIN>(phs, sws, count, op, st);
+}
+
+// Persistent TMA-staged y/x sweep: as many blocks as are resident, each taking an
+// equal share of the tiles (ceil(tiles / resident) tiles per block).
+template <int N, int AX>
+static cudaError_t launch_tma_one(const Phys& ph, const Sweep& sw, const FastOps& op, const CUtensorMap& map,
+                                  cudaStream_t st) {
+  constexpr int T = FastCfg<N, float>::T;
+  constexpr int NT = N * (N / FastCfg<N, float>::L);
+  constexpr size_t smem = TmaCfg<N>::SMEM;
+  constexpr auto kern = &k_tma_plain<N, AX>;
+  static int attr_dev = -1, resident = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    resident = (per_sm > 0 ? per_sm : 1) * sms;
+    attr_dev = dev;
+  }
+  const int per_block = (NT + resident - 1) / resident;
+  const int grid = (NT + per_block - 1) / per_block;
+  if (!op.pdl) {
+    kern<<<grid, T, smem, st>>>(ph, sw, op, map);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, ph, sw, op, map);
+}
+
+template <int N>
+cudaError_t launch_tma_n(int ax, const Phys& ph, const Sweep& sw, const FastOps& op, const CUtensorMap& map,
+                         cudaStream_t st) {
+  if (op.mode != FM_PLAIN) return cudaErrorInvalidValue;
+  if (ax == FY) return launch_tma_one<N, FY>(ph, sw, op, map, st);
+  if (ax == FX) return launch_tma_one<N, FX>(ph, sw, op, map, st);
+  return cudaErrorInvalidValue;
 }
 
 // Persistent plane-fused launch: one block per resident slot.  The scheduling

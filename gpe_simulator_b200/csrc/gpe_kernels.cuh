@@ -24,7 +24,7 @@ enum : unsigned {
 enum Axis : int { AX_Z = 0, AX_Y = 1, AX_X = 2 };
 
 // status bits
-enum : int { ST_NONFINITE = 1, ST_TIMEOUT = 2 };
+enum : int { ST_NONFINITE = 1, ST_TIMEOUT = 2, ST_LAYOUT = 4 };  // ST_LAYOUT: a sweep refused its shared-memory layout
 
 struct Phys {
   int kind;              // 0 imaginary, 1 real

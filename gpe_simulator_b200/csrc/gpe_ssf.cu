@@ -1,9 +1,12 @@
 // gpe_ssf.cu -- plans, launch sequences and the C ABI (include/gpe_ssf.h).
+#include <cuda.h>
 #include "../../include/gpe_ssf.h"
 #include "gpe_sweep.h"
 #include "gpe_fast.cuh"
 
 namespace gpe {
+cudaError_t launch_fast_tma(int n, int ax, const Phys& ph, const Sweep& sw, const FastOps& op,
+                            const CUtensorMap& map, cudaStream_t st);
 template <typename R>
 cudaError_t launch_fast(int n, int ax, const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st);
 template <typename R>
@@ -286,6 +289,11 @@ struct gpe_plan {
   bool gen = false;                // grid size needs the odd-prime radices 7/11/13
   bool fast = false;               // register-resident sweeps exist for this n
   bool plane = false;              // y and z sweeps fused per x-plane (opt-in; complex64, n = 128, 256)
+  bool tma = false;                // plain y/x sweeps stage their pencils by TMA (opt-in; complex64, n = 128, 256)
+  // tensor maps of recently swept arrays: base address -> maps of y and x tiles
+  struct TmaMaps { const void* base; CUtensorMap map[2]; };
+  TmaMaps tma_cache[4] = {};
+  int tma_next = 0;
   bool pdl_chain = false;          // inside a step sequence: sweeps may launch programmatically
   bool pdl_prev = false;           // a sweep of the current sequence has been launched
   int ept = 16;                    // elements per thread of the sweep family
@@ -419,6 +427,56 @@ int sweep(gpe_plan* p, int ax, const Sweep& sw_in, cudaStream_t st) {
 }
 
 // Register-resident sweep (n in {64, 128, 256}); same accounting as sweep().
+// cuTensorMapEncodeTiled from the driver, through the runtime's entry-point
+// query (no link-time dependency on libcuda); null when unavailable.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)f;
+  }
+  return fn;
+}
+
+// Tensor maps of the n^3 complex64 array at `base` (8-byte elements, dims z, y,
+// x innermost first): y tiles are boxes {16, n, 1}, x tiles {16, 1, n}.  Null
+// when the array cannot be staged (base not 16-byte aligned, encoder missing).
+const CUtensorMap* tma_maps(gpe_plan* p, const void* base, int fax) {
+  const int which = fax == FY ? 0 : 1;
+  for (auto& c : p->tma_cache)
+    if (c.base == base) return &c.map[which];
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc || ((uintptr_t)base & 15u)) return nullptr;
+  const cuuint64_t n = (cuuint64_t)p->n;
+  const cuuint64_t dims[3] = {n, n, n};
+  const cuuint64_t strides[2] = {n * 8, n * n * 8};
+  const cuuint32_t lt = (cuuint32_t)FastCfg<128, float>::L;
+  const cuuint32_t boxes[2][3] = {{lt, (cuuint32_t)n, 1}, {lt, 1, (cuuint32_t)n}};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  gpe_plan::TmaMaps& c = p->tma_cache[p->tma_next];
+  for (int a = 0; a < 2; ++a) {
+    const CUresult r = enc(&c.map[a], CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<void*>(base), dims, strides,
+                           boxes[a], estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      c.base = nullptr;
+      return nullptr;
+    }
+  }
+  c.base = base;
+  p->tma_next = (p->tma_next + 1) % 4;
+  return &c.map[which];
+}
+
 int fsweep(gpe_plan* p, int ax, Sweep sw, const FastOps& op, cudaStream_t st) {
   beam_centres(p, sw);
   sw.pp = p->pp;
@@ -437,8 +495,10 @@ int fsweep(gpe_plan* p, int ax, Sweep sw, const FastOps& op, cudaStream_t st) {
   FastOps o = op;
   o.pdl = p->pdl_chain && p->pdl_prev && !p->prof ? 1 : 0;
   p->pdl_prev = p->pdl_chain;
-  const cudaError_t e = p->dtype == GPE_C64 ? launch_fast<float>(p->n, fax, p->ph, sw, o, st)
-                                            : launch_fast<double>(p->n, fax, p->ph, sw, o, st);
+  const CUtensorMap* map = p->tma && o.mode == FM_PLAIN && fax != FZ ? tma_maps(p, sw.src, fax) : nullptr;
+  const cudaError_t e = map ? launch_fast_tma(p->n, fax, p->ph, sw, o, *map, st)
+                        : p->dtype == GPE_C64 ? launch_fast<float>(p->n, fax, p->ph, sw, o, st)
+                                              : launch_fast<double>(p->n, fax, p->ph, sw, o, st);
   if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("fast sweep: ") + cudaGetErrorString(e));
   ++p->launches;
   if (p->prof) {
@@ -587,6 +647,7 @@ int fill_plan(gpe_plan* p, const gpe_desc* d) {
             d->generic_only != 1 && d->dynamic_g_len == 0 && !(d->local_fp64 && d->dtype == GPE_C64) &&
             !d->exact_local;
   p->plane = p->fast && d->dtype == GPE_C64 && (n == 128 || n == 256) && d->generic_only == 3;
+  p->tma = p->fast && d->dtype == GPE_C64 && (n == 128 || n == 256) && d->generic_only == 4;
   const int emax = 512 * p->ept;
   p->lt_yx = std::max(1, std::min(d->dtype == GPE_C64 ? 16 : 8, emax / n));
   p->lt_z = std::max(1, std::min(n * n, std::min(4096, emax) / n));

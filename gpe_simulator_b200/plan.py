@@ -48,7 +48,7 @@ def _dptr(values):
 class Plan:
     def __init__(self, n, x_array, k_array, *, dtype, kind, beta, dt, kinetic_coeff=1.0,
                  static_expr="0", dynamic_expr="0", k_cut=None, beam=None, nk_bins=0,
-                 local_fp64=None, generic_only=False, fuse_planes=False, exact_local=False):
+                 local_fp64=None, generic_only=False, fuse_planes=False, exact_local=False, tma=False):
         if not torch.cuda.is_available():
             raise RuntimeError("gpe_simulator_b200 needs a CUDA device (sm_100a)")
         self.lib = _lib.load()
@@ -99,8 +99,9 @@ class Plan:
         if local_fp64 is None:
             local_fp64 = False
         d.local_fp64 = 1 if local_fp64 else 0
-        # sweep path: 0 fastest, 1 generic only, 3 y/z sweeps fused per x-plane (complex64 n = 128, 256)
-        d.generic_only = 1 if generic_only else (3 if fuse_planes else 0)
+        # sweep path: 0 fastest, 1 generic only, 3 y/z sweeps fused per x-plane (complex64 n = 128, 256),
+        # 4 fastest with the y/x pencils staged by TMA (complex64 n = 128, 256; identical results)
+        d.generic_only = 1 if generic_only else (3 if fuse_planes else (4 if tma else 0))
         # exact local sub-flows: an accuracy mode that departs from the reference on purpose
         d.exact_local = 1 if exact_local else 0
         self.local_fp64 = bool(local_fp64)
@@ -259,7 +260,8 @@ class Plan:
         return out
 
     def status(self):
-        """Device status bits (1 = non-finite norm, 2 = timeout); clears them."""
+        """Device status bits (1 = non-finite norm, 2 = timeout, 4 = a sweep refused its
+        shared-memory layout); clears them."""
         flags = ctypes.c_int()
         _lib.check(self.lib.gpe_status(self._h, ctypes.byref(flags), _stream()))
         return flags.value

@@ -122,7 +122,11 @@ typedef struct gpe_desc {
      * 2 = same as 0; 3 = complex64 n = 128, 256: the y and z sweeps of each
      * x-plane fused into one persistent launch (psi crosses HBM once per launch
      * instead of once per sweep; identical results, measured slower on B200
-     * because the sweeps are issue-bound, not HBM-bound). */
+     * because the sweeps are issue-bound, not HBM-bound); 4 = as 0, and
+     * complex64 n = 128, 256 stage the pencils of their plain y/x sweeps by TMA
+     * in persistent double-buffered launches (identical results; the y sweep
+     * times the same alone, and the step is 4-5% slower because a persistent
+     * grid ends the overlap of neighbouring launches). */
     int generic_only;
     /* 1 = exact local sub-flows (an accuracy mode that departs from the reference
      * on purpose; evaluated in FP64 on the generic sweeps): imaginary time
@@ -190,7 +194,8 @@ int  gpe_launch_count(const gpe_plan* plan, long long* count);
 int  gpe_profile(gpe_plan* plan, int enable);
 int  gpe_profile_read(gpe_plan* plan, double* ms, long long* count);
 
-/* device status word: bit 0 non-finite norm, bit 1 timeout; read and clear (synchronises) */
+/* device status word: bit 0 non-finite norm, bit 1 timeout, bit 2 a sweep refused its
+ * shared-memory layout (its tiles were not transformed); read and clear (synchronises) */
 int  gpe_status(gpe_plan* plan, int* flags, void* stream);
 
 /* Batches: many independent imaginary-time solves (mixed grid sizes, one dtype)

@@ -88,6 +88,39 @@ def test_plane_fused_equals_unfused_bitwise(cuda, n, kind):
     assert fused.status() == 0 and plain.status() == 0
 
 
+@pytest.mark.parametrize("n", [128, 256])
+@pytest.mark.parametrize("kind", ["imaginary", "real"])
+def test_tma_staged_sweeps_equal_plain_loads_bitwise(cuda, n, kind):
+    """The y/x sweeps whose pencils arrive by TMA (persistent, double-buffered)
+    run the arithmetic of the register-resident sweeps with plain loads:
+    identical bits for step sequences, out-of-place transforms (x sweeps, source
+    != destination), and a state whose address is not 16-byte aligned (staging
+    is skipped there)."""
+    from gpe_simulator_b200 import Beam
+    kw = dict(beta=800.0, dt=4e-4, static_expr=cases.TRAP)
+    if kind == "real":
+        kw["beam"] = Beam(20.0, 0.5, 2.0, 1.0, 0.004)
+    staged, x = make(n, 12.0, kind, torch.complex64, False, tma=True, **kw)
+    plain, _ = make(n, 12.0, kind, torch.complex64, False, **kw)
+    a = torch.from_numpy(ssf.noisy_gaussian(x, seed=n + 1)).to(torch.complex64).cuda()
+    b = a.clone()
+    for s0, k in ((0, 5), (5, 1), (6, 4)):
+        staged.step(a, k, s0)
+        plain.step(b, k, s0)
+    assert torch.equal(a, b)
+    fa, fb = staged.fft(a), plain.fft(b)
+    assert torch.equal(fa, fb)
+    assert torch.equal(staged.fft(fa, inverse=True), plain.fft(fb, inverse=True))
+    # an 8-byte offset view: the tensor map would not be 16-byte aligned
+    buf = torch.zeros(n ** 3 + 1, dtype=torch.complex64, device="cuda")
+    c = buf[1:].view(n, n, n)
+    c.copy_(a)
+    staged.step(c, 3, 10)
+    plain.step(b, 3, 10)
+    assert torch.equal(c, b)
+    assert staged.status() == 0 and plain.status() == 0
+
+
 @pytest.mark.parametrize("kind", ["imaginary", "real"])
 def test_fast_512_matches_generic(cuda, kind):
     """512^3 complex64 (the largest single solve): register-resident sweeps vs
