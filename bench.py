@@ -48,6 +48,9 @@ KERNELS = {"z": "k_fast_occ<256, 0, float, 3, 3> (fused z sweep)",
            "y": "k_fast_occ<256, 1, float, 0, 4> (y sweep, 2 per step)",
            "x": "k_fast_occ<256, 2, float, 4, 3> (x sweep with kinetic phase)"}
 TRAFFIC_KEYS = {"z": "sweep_z", "y": "sweep_y", "x": "sweep_x"}
+# opt-in sweep paths (identical results): the kernels that replace the default ones
+PATH_KERNELS = {"tma": {"y": ("k_tma_plain<256, 1> (TMA-staged y sweep, 2 per step)", "sweep_y_tma")},
+                "plane": {"z": ("k_plane<256, float, 3> (inverse y, Z21, forward y per x-plane)", "plane")}}
 
 
 def measured_peak():
@@ -184,7 +187,7 @@ def ours(args, world, rank, local):
     beam = beam_in_reference_units(BEAM["amp"], BEAM["width"], BEAM["radius"], BEAM["omega"],
                                    BEAM["ramp_steps"] * DT)
     plan = Plan(N_GRID, x, k, dtype=torch.complex64, kind="real", beta=2 * G, dt=DT / 2,
-                static_expr=TRAP_REF, beam=beam)
+                static_expr=TRAP_REF, beam=beam, tma=args.path == "tma", fuse_planes=args.path == "plane")
     prep = Plan(N_GRID, x, k, dtype=torch.complex64, kind="imaginary", beta=2 * G, dt=DT,
                 static_expr=TRAP_REF)
     host0 = initial_state(x, seed=rank).astype(np.complex64)
@@ -224,10 +227,13 @@ def ours(args, world, rank, local):
     bytes_per_launch = 2 * s_bytes * m
     achieved = bytes_per_launch / (dom_ms / dom_n / 1e3) / 1e9
     peak, peak_kind = measured_peak()
+    kernel, tkey = KERNELS[dom], TRAFFIC_KEYS[dom]
+    if dom in PATH_KERNELS.get(args.path, {}):
+        kernel, tkey = PATH_KERNELS[args.path][dom]
     traffic = None
     tfile = ROOT / "profiles" / "traffic.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(TRAFFIC_KEYS[dom])
+        traffic = json.loads(tfile.read_text()).get(tkey)
 
     # ---- end to end: public closure API with host buffers, H2D + D2H every step
     from gpe_simulator_b200.make_propagator import make_real_propagator
@@ -290,10 +296,11 @@ def ours(args, world, rank, local):
         "data": "synthetic (seeded noisy Gaussian relaxed 50 imaginary steps)",
         "config": {"workload": WORKLOAD, "grid": N_GRID, "psi_bytes": nbytes,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "sweep_path": args.path,
                    "l2": "inputs larger than L2 (128 MiB psi vs 126 MB L2), no flush"},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "kernel": KERNELS[dom],
+                     "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                      "traffic_source": "profiles/traffic.json (ncu dram bytes read + write per launch)",
                      "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_per_launch,
@@ -479,6 +486,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 512^3 leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--path", choices=("default", "tma", "plane"), default="default",
+                    help="sweep path of the main leg: default, tma (y/x pencils staged by TMA), "
+                         "plane (y/z sweeps fused per x-plane); identical results")
     ap.add_argument("--serve-requests", type=int, default=120)
     ap.add_argument("--serve-rate", type=float, default=50.0)
     args = ap.parse_args()

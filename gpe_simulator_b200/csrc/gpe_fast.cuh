@@ -90,6 +90,13 @@ template <int N, typename R> __host__ __device__ constexpr size_t fast_tables_by
          / 16 * 16;
 }
 
+// the same at run time (host): the shell histogram of a diagnostic x sweep lives
+// in the tables region, so it holds at most this many bytes of bins
+inline size_t fast_tables_bytes_rt(int n, int real_bytes) {
+  const int L = n == 512 ? 8 : (real_bytes == 4 ? 16 : 8);
+  return (((size_t)(n + L) * (16 + 8) + (size_t)(n + 3 * L) * real_bytes) + 15) / 16 * 16;
+}
+
 // shared memory of a fast sweep (bytes)
 template <int N, typename R> __host__ __device__ constexpr size_t fast_smem_bytes() {
   return (size_t)(2 * N) * sizeof(typename Cx<R>::T)
@@ -208,7 +215,7 @@ __device__ __forceinline__ void scale_all(C (&v)[EPT], R f) {
   for (int q = 0; q < EPT; ++q) { v[q].x *= f; v[q].y *= f; }
 }
 
-enum : int { FM_PLAIN = 0, FM_Z1 = 1, FM_Z2 = 2, FM_Z21 = 3, FM_XKIN = 4 };
+enum : int { FM_PLAIN = 0, FM_Z1 = 1, FM_Z2 = 2, FM_Z21 = 3, FM_XKIN = 4, FM_DIAGR = 5, FM_DIAGK = 6 };
 
 // sin(x) and cos(x) - 1 from their Taylor series (Horner, FP32), valid for
 // |x| <= pi/4 where the first omitted terms (x^13/13!, x^14/14!) are below 1e-11;
@@ -452,6 +459,72 @@ __device__ __forceinline__ void half_dispatch(typename Cx<R>::T (&v)[EPT], const
   }
 }
 
+// Diagnostic real-space sums of psi at time cx.t1 on the registers (layout LANES
+// x VALS, element m = lane + LANES*a of line l), the terms of the reference's
+// get_N and of E_pot, E_int (gpe/helper.py:81-93, 123-140): |psi|^2, V |psi|^2,
+// |psi|^4 with the potential of the generic sweeps; a thread's values summed in
+// plain FP64, the thread sums added with compensation.
+template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT>
+__device__ __forceinline__ void diag_real_all(const typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
+                                              const Phys& ph, PwCtx<R>& cx) {
+  constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
+#pragma unroll
+  for (int s = 0; s < SLOTS; ++s) {
+    if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
+    int l, lane;
+    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+    double n0 = 0.0, n1 = 0.0, n2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < VALS; ++a) {
+      const int m = lane + LANES * a;
+      int i, j, k;
+      tl.coords(l, m, i, j, k);
+      const typename Cx<R>::T x = v[s * VALS + a];
+      const double rho = (double)x.x * x.x + (double)x.y * x.y;
+      const double V = (double)potential<R>(ph, N, i, j, k, tl.gidx(l, m), cx.t1, cx.b1x, cx.b1y);
+      n0 += rho;
+      n1 = fma(V, rho, n1);
+      n2 = fma(rho, rho, n2);
+    }
+    cx.acc[0].add(n0);
+    cx.acc[1].add(n1);
+    cx.acc[2].add(n2);
+  }
+}
+
+// Diagnostic k-space sums of the transformed state (layout LANES x VALS after
+// the x transform, frequency index m = lane + LANES*a): sum k^2 |psi_k|^2 (the
+// reference's get_E) and, when cx.hist is set, the shell histogram of |psi_k|^2
+// (gpe/nk_extraction.py:5-21); k^2 and the shell rule as in the generic sweeps.
+template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT>
+__device__ __forceinline__ void diag_k_all(const typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
+                                           const Phys& ph, PwCtx<R>& cx) {
+  constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
+#pragma unroll
+  for (int s = 0; s < SLOTS; ++s) {
+    if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
+    int l, lane;
+    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+    double e = 0.0;
+#pragma unroll
+    for (int a = 0; a < VALS; ++a) {
+      const int m = lane + LANES * a;
+      int i, j, k;
+      tl.coords(l, m, i, j, k);
+      const typename Cx<R>::T x = v[s * VALS + a];
+      const double kk = ph.k[i] * ph.k[i] + ph.k[j] * ph.k[j] + ph.k[k] * ph.k[k];
+      const double w = (double)x.x * x.x + (double)x.y * x.y;
+      e = fma(kk, w, e);
+      if (cx.hist) {
+        int sh = (int)floor(sqrt(kk) / cx.shell_w + 0.5);
+        sh = min(sh, cx.nbins - 1);
+        atomicAdd(cx.hist + sh, w);
+      }
+    }
+    cx.acc[3].add(e);
+  }
+}
+
 // Pointwise stages of the fast modes on registers in layout (LANES lanes, VALS values).
 template <int N, int AX, typename R, int MODE, int STAGE, int LANES, int VALS, int SLOTS, int EPT>
 __device__ __forceinline__ void fast_pointwise(typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
@@ -547,6 +620,8 @@ __device__ __forceinline__ void fast_store(const typename Cx<R>::T (&v)[EPT], co
 //   FM_Z2     inverse, 1/M, half(t1) [norm partials]                last z sweep of a step
 //   FM_Z21    inverse, 1/M, half(t1), half(t2), forward             last z of a step + first z of the next
 //   FM_XKIN   forward, kinetic, inverse                             x sweep
+//   FM_DIAGR  real-space sums (N, E_pot, E_int), forward            diagnostic z sweep (to the work buffer)
+//   FM_DIAGK  forward, k-space sums (E_kin [, shells]), no store     diagnostic x sweep
 template <int N, int AX, typename R, int MODE, bool CG = false>
 __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const FastOps& op, int tile,
                                           int ntiles) {
@@ -596,6 +671,9 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
     }
     if (ZM) z_tables<N, R>(ph, sw, tl.a0, tb, MODE == FM_Z21);
     if (MODE == FM_XKIN) x_tables<N, R>(ph, tl.a0, tl.b0, tb);
+    // diagnostic x sweep: the shell histogram takes the tables region
+    if (MODE == FM_DIAGK && sw.hist)
+      for (int b = threadIdx.x; b < sw.nbins; b += T) ((double*)tail)[b] = 0.0;
   };
   // psi and the renormalisation scale come from the previous sweep: read them
   // after the grid-dependency wait; the tile's loads are issued first and are in
@@ -609,12 +687,23 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
     cx.sc_div = __ldcg(sw.scale);
     cx.sc_mul = (R)__ldcg(sw.scale + 1);
   }
+  if (MODE == FM_DIAGR) {
+    cx.t1 = sw.t1;
+    cx.b1x = sw.bc1x;
+    cx.b1y = sw.bc1y;
+  }
+  if (MODE == FM_DIAGK) {
+    cx.hist = sw.hist ? (double*)tail : nullptr;
+    cx.nbins = sw.nbins;
+    cx.shell_w = sw.shell_w;
+  }
 
   C v[EPT];
   fast_load<N, AX, R, S1, CG>(v, tl, (const C*)sw.src, MODE == FM_Z2 || MODE == FM_Z21 || (MODE == FM_PLAIN && op.inv1));
   prologue();
   __syncthreads();  // twiddles and tables visible
   if (MODE == FM_Z1) fast_pointwise<N, AX, R, MODE, 0, N1, N2, S1>(v, tl, ph, tb, op, cx);
+  if (MODE == FM_DIAGR) diag_real_all<N, AX, R, N1, N2, S1>(v, tl, ph, cx);
   fft_2phase<N, N1, N2, AX, R, S1, S2, EPT>(v, ex, t1);
   if (MODE == FM_Z21 || MODE == FM_XKIN) {
     if (MODE == FM_Z21) conj_all(v);  // finish the inverse before the physics
@@ -627,12 +716,24 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
     if (MODE == FM_Z2 || (MODE == FM_PLAIN && op.inv1)) conj_all(v);
     if (MODE == FM_Z2) fast_pointwise<N, AX, R, MODE, 2, N2, N1, S2>(v, tl, ph, tb, op, cx);
     if (MODE == FM_PLAIN && op.invm) scale_all(v, (R)ph.inv_m);
-    fast_store<N, AX, R, N2, N1, S2>(v, tl, (C*)sw.dst);
+    if (MODE == FM_DIAGK) diag_k_all<N, AX, R, N2, N1, S2>(v, tl, ph, cx);
+    else fast_store<N, AX, R, N2, N1, S2>(v, tl, (C*)sw.dst);
   }
   if (MODE == FM_Z2 && op.norm) {
     Acc a[1] = {cx.acc[0]};
     block_merge<1>(a, red);
     norm_finish_n(ph, sw, a[0], red, tile, ntiles);
+  }
+  if (MODE == FM_DIAGR || MODE == FM_DIAGK) {
+    // per-tile partials in the generic sweeps' layout: [tile][N, E_pot, E_int, E_kin]
+    Acc a[4] = {cx.acc[0], cx.acc[1], cx.acc[2], cx.acc[3]};
+    block_merge<4>(a, red);
+    if (threadIdx.x == 0)
+      for (int q = 0; q < 4; ++q) sw.partial[(long long)tile * 4 + q] = a[q].value();
+    if (MODE == FM_DIAGK && sw.hist) {
+      __syncthreads();
+      for (int b = threadIdx.x; b < sw.nbins; b += T) sw.hist[(long long)tile * sw.nbins + b] = cx.hist[b];
+    }
   }
 }
 
@@ -642,9 +743,10 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
 // T = 256); the fused modes keep 768 (85 registers) for their extra live state.
 // At n = 512 (32-point phase, up to 214 registers unbounded) 768 / 512 threads
 // per SM: 240 -> 291 steps/s at 512^3 despite a few hundred bytes of spills.
+// The diagnostic z sweep (FP64 potential per point) keeps 512 threads per SM.
 template <int N, typename R, int MODE> struct FastBounds {
   static constexpr int value = (sizeof(R) == 4 && (N == 128 || N == 256))
-                                   ? (MODE == FM_PLAIN ? 1024 : 768) / FastCfg<N, R>::T
+                                   ? (MODE == FM_PLAIN ? 1024 : MODE == FM_DIAGR ? 512 : 768) / FastCfg<N, R>::T
                                : (sizeof(R) == 4 && N == 512)
                                    ? (MODE == FM_PLAIN ? 768 : 512) / FastCfg<N, R>::T : 0;
 };

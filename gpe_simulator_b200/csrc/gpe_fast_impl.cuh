@@ -57,6 +57,8 @@ cudaError_t launch_fast_n(int ax, const Phys& ph, const Sweep& sw, const FastOps
     case FM_Z2: return launch_fast_one<N, FZ, R, FM_Z2>(ph, sw, op, st);
     case FM_Z21: return launch_fast_one<N, FZ, R, FM_Z21>(ph, sw, op, st);
     case FM_XKIN: return launch_fast_one<N, FX, R, FM_XKIN>(ph, sw, op, st);
+    case FM_DIAGR: return launch_fast_one<N, FZ, R, FM_DIAGR>(ph, sw, op, st);
+    case FM_DIAGK: return launch_fast_one<N, FX, R, FM_DIAGK>(ph, sw, op, st);
     default: break;
   }
   if (ax == FZ) return launch_fast_one<N, FZ, R, FM_PLAIN>(ph, sw, op, st);
@@ -92,6 +94,8 @@ cudaError_t launch_fastb_n(int ax, const Phys* phs, const Sweep* sws, int count,
     case FM_Z2: return launch_fastb_one<N, FZ, R, FM_Z2>(phs, sws, count, op, st);
     case FM_Z21: return launch_fastb_one<N, FZ, R, FM_Z21>(phs, sws, count, op, st);
     case FM_XKIN: return launch_fastb_one<N, FX, R, FM_XKIN>(phs, sws, count, op, st);
+    case FM_DIAGR: return launch_fastb_one<N, FZ, R, FM_DIAGR>(phs, sws, count, op, st);
+    case FM_DIAGK: return launch_fastb_one<N, FX, R, FM_DIAGK>(phs, sws, count, op, st);
     default: break;
   }
   if (ax == FZ) return launch_fastb_one<N, FZ, R, FM_PLAIN>(phs, sws, count, op, st);

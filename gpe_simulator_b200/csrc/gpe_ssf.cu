@@ -165,8 +165,7 @@ __global__ void k_build_static(int n, const double* x, const double* prog, int l
 
 // Sum per-block diagnostic partials in a fixed order.
 // out[0..3] = sums of pa columns 0..2 and pb column 3; out[4 + b] = histogram bin b.
-__global__ void k_finish_diag(const double* pa, int na, const double* pb, int nb, const double* hist,
-                              int nbins, double* out) {
+__global__ void k_finish_diag(const double* pa, int na, const double* pb, int nb, double* out) {
   __shared__ Acc sh[32 * 4];
   Acc a[4];
   for (int b = threadIdx.x; b < na; b += blockDim.x) {
@@ -178,13 +177,58 @@ __global__ void k_finish_diag(const double* pa, int na, const double* pb, int nb
   block_merge<4>(a, sh);
   if (threadIdx.x == 0)
     for (int v = 0; v < 4; ++v) out[v] = a[v].value();
-  if (hist) {
-    for (int bin = threadIdx.x; bin < nbins; bin += blockDim.x) {
-      Acc h;
-      for (int b = 0; b < nb; ++b) h.add(hist[(long long)b * nbins + bin]);
-      out[4 + bin] = h.value();
-    }
+}
+
+// Shell histograms: block `bin` sums that bin over the nb per-tile histograms
+// (threads stride over the tiles with compensation, merged in a fixed order)
+// into out[4 + bin].
+__global__ void k_finish_hist(const double* hist, int nb, int nbins, double* out) {
+  __shared__ Acc sh[32];
+  const int bin = blockIdx.x;
+  Acc a[1];
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) a[0].add(hist[(long long)b * nbins + bin]);
+  block_merge<1>(a, sh);
+  if (threadIdx.x == 0) out[4 + bin] = a[0].value();
+}
+
+// Lagged renormalisation of a whole state with the pending scale (the
+// arithmetic of PW_SCALE: complex64 times (float)(1/sqrt N), complex128 divided
+// by sqrt N), elementwise: a thread takes 4 elements, a warp 4 runs of 32.
+template <typename R>
+__device__ __forceinline__ void scale_state(typename Cx<R>::T* psi, long long count, const double* scale) {
+  using C = typename Cx<R>::T;
+  const long long e0 = (long long)blockIdx.x * blockDim.x * 4 + threadIdx.x;
+  C v[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long e = e0 + (long long)q * blockDim.x;
+    v[q] = e < count ? psi[e] : mk((R)0, (R)0);
   }
+  if (sizeof(R) == 4) {
+    const R f = (R)__ldcg(scale + 1);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { v[q].x *= f; v[q].y *= f; }
+  } else {
+    const double d = __ldcg(scale);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { v[q].x = (R)((double)v[q].x / d); v[q].y = (R)((double)v[q].y / d); }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long e = e0 + (long long)q * blockDim.x;
+    if (e < count) psi[e] = v[q];
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_scale(Sweep sw, long long count) {
+  scale_state<R>((typename Cx<R>::T*)sw.dst, count, sw.scale);
+}
+
+// batched: blockIdx.y selects the instance
+template <typename R>
+__global__ void __launch_bounds__(256) k_scale_batch(const Sweep* __restrict__ sws, long long count) {
+  scale_state<R>((typename Cx<R>::T*)sws[blockIdx.y].dst, count, sws[blockIdx.y].scale);
 }
 
 // Batched finish: block b sums the partials of instance jobs[b] into out[4*index].
@@ -426,7 +470,6 @@ int sweep(gpe_plan* p, int ax, const Sweep& sw_in, cudaStream_t st) {
   return rc;
 }
 
-// Register-resident sweep (n in {64, 128, 256}); same accounting as sweep().
 // cuTensorMapEncodeTiled from the driver, through the runtime's entry-point
 // query (no link-time dependency on libcuda); null when unavailable.
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -477,6 +520,7 @@ const CUtensorMap* tma_maps(gpe_plan* p, const void* base, int fax) {
   return &c.map[which];
 }
 
+// Register-resident sweep (n with a fast split); same accounting as sweep().
 int fsweep(gpe_plan* p, int ax, Sweep sw, const FastOps& op, cudaStream_t st) {
   beam_centres(p, sw);
   sw.pp = p->pp;
@@ -587,8 +631,14 @@ int norm_sweep(gpe_plan* p, const void* psi, cudaStream_t st) {
 
 int scale_sweep(gpe_plan* p, void* psi, cudaStream_t st) {
   Sweep s = mk_sweep(psi, psi);
-  s.pre = PW_SCALE;
-  return sweep(p, AX_Z, s, st);
+  s.scale = p->d_scale;
+  const long long count = (long long)p->n * p->n * p->n;
+  const unsigned blocks = (unsigned)((count + 1023) / 1024);
+  if (p->dtype == GPE_C64) k_scale<float><<<blocks, 256, 0, st>>>(s, count);
+  else k_scale<double><<<blocks, 256, 0, st>>>(s, count);
+  CU(cudaGetLastError());
+  ++p->launches;
+  return GPE_OK;
 }
 
 int ensure_work(gpe_plan* p) {
@@ -600,7 +650,8 @@ int ensure_work(gpe_plan* p) {
 
 int ensure_hist(gpe_plan* p) {
   if (p->d_hist) return GPE_OK;
-  const size_t bytes = (size_t)tiles_of(p, AX_X) * p->nbins * sizeof(double);
+  // per-tile histograms of the generic or the register-resident x sweep
+  const size_t bytes = (size_t)p->max_tiles * p->nbins * sizeof(double);
   CU(cudaMalloc(&p->d_hist, bytes));
   return GPE_OK;
 }
@@ -922,10 +973,9 @@ int kspace_reduce(gpe_plan* p, const void* f, cudaStream_t st) {
   return sweep(p, AX_X, s, st);
 }
 
-int finish_diag(gpe_plan* p, int na, bool hist, std::vector<double>& host, cudaStream_t st) {
-  const int nb = tiles_of(p, AX_X);
-  k_finish_diag<<<1, 256, 0, st>>>(p->d_partial, na, p->d_partial + 4 * (size_t)p->max_tiles, nb,
-                                   hist ? p->d_hist : nullptr, p->nbins, p->d_out);
+int finish_diag(gpe_plan* p, int na, int nb, bool hist, std::vector<double>& host, cudaStream_t st) {
+  k_finish_diag<<<1, 256, 0, st>>>(p->d_partial, na, p->d_partial + 4 * (size_t)p->max_tiles, nb, p->d_out);
+  if (hist) k_finish_hist<<<p->nbins, 256, 0, st>>>(p->d_hist, nb, p->nbins, p->d_out);
   CU(cudaGetLastError());
   host.assign(4 + p->nbins, 0.0);
   CU(cudaMemcpyAsync(host.data(), p->d_out, host.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -936,7 +986,39 @@ int finish_diag(gpe_plan* p, int na, bool hist, std::vector<double>& host, cudaS
 // The three diagnostic sweeps of psi at time t (real-space sums in the z sweep
 // writing the partial transform to the plan's work buffer, k-space sums and
 // shells in the x sweep); results stay on the device until finish_diag.
-int diag_launch(gpe_plan* p, const void* psi, double t, cudaStream_t st) {
+// Tile counts of the diagnostic z and x sweeps (the partials to finish).
+void diag_tiles(const gpe_plan* p, bool fast, int& na, int& nb) {
+  if (fast) {
+    const int lt = p->n == 512 ? 8 : (p->dtype == GPE_C64 ? 16 : 8);
+    na = p->n * p->n / lt;
+    nb = p->n * (p->n / lt);
+  } else {
+    na = tiles_of(p, AX_Z);
+    nb = tiles_of(p, AX_X);
+  }
+}
+
+// The diagnostics run on the register-resident sweeps when the plan has them
+// and the shell histogram (if wanted) fits their shared tables region.
+bool diag_fast(const gpe_plan* p, bool hist) {
+  return p->fast && (!hist || (size_t)p->nbins * sizeof(double) <= fast_tables_bytes_rt(p->n, (int)p->csize / 2));
+}
+
+int diag_launch(gpe_plan* p, const void* psi, double t, bool hist, cudaStream_t st) {
+  if (diag_fast(p, hist)) {
+    Sweep s = mk_sweep(psi, p->d_work);
+    s.t1 = t;
+    s.partial = p->d_partial;
+    TRY(fsweep(p, AX_Z, s, mk_ops(FM_DIAGR), st));
+    s = mk_sweep(p->d_work, p->d_work);
+    TRY(fsweep(p, AX_Y, s, mk_ops(FM_PLAIN), st));
+    s = mk_sweep(p->d_work, nullptr);
+    s.partial = p->d_partial + 4 * (size_t)p->max_tiles;
+    s.hist = hist ? p->d_hist : nullptr;
+    s.nbins = p->nbins;
+    s.shell_w = p->shell_w;
+    return fsweep(p, AX_X, s, mk_ops(FM_DIAGK), st);
+  }
   Sweep s = mk_sweep(psi, p->d_work);
   s.pre = PW_DIAG_R;
   s.t1 = t;
@@ -1199,7 +1281,7 @@ int gpe_kinetic_energy(gpe_plan* p, const void* psi_k, double* e_kin, void* stre
   cudaStream_t st = (cudaStream_t)stream;
   TRY(kspace_reduce(p, psi_k, st));
   std::vector<double> h;
-  TRY(finish_diag(p, 0, false, h, st));
+  TRY(finish_diag(p, 0, tiles_of(p, AX_X), false, h, st));
   *e_kin = h[3] * p->ph.dx3 * p->ph.inv_m;
   return GPE_OK;
 }
@@ -1209,7 +1291,7 @@ int gpe_nk_extraction(gpe_plan* p, const void* psi_k, double* occupation, long l
   cudaStream_t st = (cudaStream_t)stream;
   TRY(kspace_reduce(p, psi_k, st));
   std::vector<double> h;
-  TRY(finish_diag(p, 0, true, h, st));
+  TRY(finish_diag(p, 0, tiles_of(p, AX_X), true, h, st));
   const double f = p->ph.dx3 * p->ph.inv_m;
   if (occupation)
     for (int b = 0; b < p->nbins; ++b) occupation[b] = h[4 + b] * f;
@@ -1224,10 +1306,12 @@ int gpe_diagnostics(gpe_plan* p, const void* psi, double t, double* scalars, dou
   cudaStream_t st = (cudaStream_t)stream;
   TRY(ensure_work(p));
   TRY(ensure_hist(p));
-  TRY(diag_launch(p, psi, t, st));
-  const int na = tiles_of(p, AX_Z);
+  const bool hist = nk != nullptr;
+  TRY(diag_launch(p, psi, t, hist, st));
+  int na = 0, nb = 0;
+  diag_tiles(p, diag_fast(p, hist), na, nb);
   std::vector<double> h;
-  TRY(finish_diag(p, na, nk != nullptr, h, st));
+  TRY(finish_diag(p, na, nb, hist, h, st));
   diag_scalars(p, h.data(), scalars);
   if (nk)
     for (int b = 0; b < p->nbins; ++b) nk[b] = h[4 + b] * p->ph.dx3 * p->ph.inv_m;
@@ -1372,8 +1456,9 @@ Sweep role_sweep(int role, void* psi, gpe_plan* p) {
     case ROLE_DZ: s.dst = p->d_work; s.pre = PW_DIAG_R; s.fft1 = 1; s.t1 = 0.0; break;
     case ROLE_DY: s.src = p->d_work; s.dst = p->d_work; s.fft1 = 1; break;
     default:
+      // (the register-resident x sweep skips the shell histogram: batches finish energies only)
       s.src = p->d_work; s.dst = nullptr; s.fft1 = 1; s.post = PW_DIAG_K;
-      s.partial = p->d_partial + 4 * (size_t)p->max_tiles; s.hist = p->d_hist;
+      s.partial = p->d_partial + 4 * (size_t)p->max_tiles; s.hist = diag_fast(p, false) ? nullptr : p->d_hist;
       break;
   }
   return s;
@@ -1392,7 +1477,15 @@ int group_launch(gpe_batch* b, gpe_batch::Group& g, int role, cudaStream_t st) {
   if (g.uploaded != count) return fail(GPE_ERR_ARG, "batch membership changed without gpe_batch_bind");
   const Sweep* sws = g.d_sw + (size_t)role * count;
   const int ax = role_axis(role);
-  if (g.fast && role < ROLE_SC) {
+  if (role == ROLE_SC) {
+    // lagged renormalisation: an elementwise pass per instance
+    const long long elems = (long long)g.n * g.n * g.n;
+    k_scale_batch<R><<<dim3((unsigned)((elems + 1023) / 1024), (unsigned)count), 256, 0, st>>>(sws, elems);
+    CU(cudaGetLastError());
+    ++b->launches;
+    return GPE_OK;
+  }
+  if (g.fast) {
     FastOps op = mk_ops(FM_PLAIN);
     const int fax = ax == AX_Z ? FZ : ax == AX_Y ? FY : FX;
     switch (role) {
@@ -1401,6 +1494,9 @@ int group_launch(gpe_batch* b, gpe_batch::Group& g, int role, cudaStream_t st) {
       case ROLE_Y1: op = mk_ops(FM_PLAIN); break;
       case ROLE_X: op = mk_ops(FM_XKIN); break;
       case ROLE_Y2: op = mk_ops(FM_PLAIN, 1); break;
+      case ROLE_DZ: op = mk_ops(FM_DIAGR); break;
+      case ROLE_DY: op = mk_ops(FM_PLAIN); break;
+      case ROLE_DX: op = mk_ops(FM_DIAGK); break;
       default: op = mk_ops(FM_Z2, 0, 0, 0, 1); break;
     }
     CU(launch_fast_batch<R>(g.n, fax, g.d_ph, sws, count, op, st));
@@ -1488,8 +1584,7 @@ int jobs_upload(gpe_batch* b) {
       DiagJob j;
       j.pa = p->d_partial;
       j.pb = p->d_partial + 4 * (size_t)p->max_tiles;
-      j.na = tiles_of(p, AX_Z);
-      j.nb = tiles_of(p, AX_X);
+      diag_tiles(p, diag_fast(p, false), j.na, j.nb);
       j.index = i;
       jobs.push_back(j);
     }

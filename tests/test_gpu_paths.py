@@ -42,6 +42,46 @@ def test_fast_matches_generic_and_oracle(cuda, n, dtype, tol, kind):
 
 
 @pytest.mark.parametrize("n", [32, 48, 64, 96, 128, 160, 256])
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+@pytest.mark.parametrize("kind", ["imaginary", "real"])
+def test_fast_diagnostics_match_generic_and_oracle(cuda, n, dtype, kind):
+    """Diagnostics on the register-resident sweeps (z: real-space sums and the
+    forward transform; y; x: forward transform, sum k^2 |psi_k|^2 and the shell
+    histogram) against the generic sweeps and the oracle on the same state at a
+    time where the beam has moved.  Both paths agree to 1e-12 on the sums of
+    psi itself (N, E_pot, E_int); against the oracle, complex64 E_pot carries
+    the FP32 evaluation of the potential (1e-8) and E_kin and n(k) the FP32
+    transform's rounding."""
+    from gpe_simulator_b200 import Beam
+    kw = dict(beta=800.0, dt=4e-4, static_expr=cases.TRAP)
+    if kind == "real":
+        kw["beam"] = Beam(20.0, 0.5, 2.0, 1.0, 0.004)
+    fast, x = make(n, 12.0, kind, dtype, False, **kw)
+    slow, _ = make(n, 12.0, kind, dtype, True, **kw)
+    psi = torch.from_numpy(ssf.noisy_gaussian(x, seed=n)).to(dtype).cuda()
+    t = 0.003
+    a, b = fast.diagnostics(psi, t=t, nk=True), slow.diagnostics(psi, t=t, nk=True)
+    c128 = dtype == torch.complex128
+    m = ssf.Model(n=n, simulation_range=12.0, kind=kind, beta=800.0, dt=4e-4, static_expr=cases.TRAP,
+                  beam=ssf.Beam(20.0, 0.5, 2.0, 1.0, 0.004) if kind == "real" else None)
+    state = psi.cpu().numpy()
+    want = ssf.energies(state, m, t=t)
+    spec = ssf.nk_extraction(np.fft.fftn(state.astype(np.complex128)), x, m.k)
+    for key in ("N", "E_pot", "E_int", "E_kin", "E", "mu"):
+        same = 1e-12 if (c128 or key in ("N", "E_pot", "E_int")) else 1e-6
+        assert a[key] == pytest.approx(b[key], rel=same), (key, a[key], b[key])
+        oracle = 1e-12 if (c128 or key in ("N", "E_int")) else (1e-7 if key == "E_pot" else 1e-6)
+        assert a[key] == pytest.approx(want[key], rel=oracle), (key, a[key], want[key])
+    np.testing.assert_array_equal(a["counts"], spec["counts"])
+    np.testing.assert_allclose(a["Nk"], spec["Nk"], rtol=1e-10 if c128 else 1e-5,
+                               atol=(1e-14 if c128 else 1e-8) * spec["Nk"].max())
+    # energies alone (no shell histogram) give the same sums
+    e = fast.diagnostics(psi, t=t)
+    assert all(e[key] == a[key] for key in ("N", "E_kin", "E_pot", "E_int"))
+    assert fast.status() == 0
+
+
+@pytest.mark.parametrize("n", [32, 48, 64, 96, 128, 160, 256])
 def test_fast_fft_matches_numpy(cuda, n):
     p, _ = make(n, 10.0, "imaginary", torch.complex64, False, beta=0.0, dt=0.0)
     g = torch.Generator(device="cuda").manual_seed(n)
