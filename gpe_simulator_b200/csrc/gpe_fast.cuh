@@ -36,12 +36,22 @@ template <> struct Split<512> { static constexpr int N1 = 32, N2 = 16; };
 
 __host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
 
-// Lines per tile L (128-byte rows for y/x tiles; 64-byte for 512) and threads per
+// Lines per tile L (128-byte rows for y/x tiles) and threads per
 // block T.  The layout (N1 lanes, N2 values) has P1 = L*N1 slots, (N2 lanes, N1
 // values) has P2 = L*N2; a thread holds Q1 (resp. Q2) slots, some threads idle in
 // one phase when P1 != P2 do not divide evenly.
+// lines per tile of the register-resident sweeps (host and device): 16 for
+// complex64 (128-byte rows in y/x tiles), 8 for complex128 (also 128 bytes).
+// At n = 512 (complex64 only) 16 lines take 512 threads; measured against 8
+// lines (256 threads, 64-byte rows): 291 -> 312 steps/s at 512^3, the gain
+// being in the overlap of programmatically launched sweeps (per-launch times
+// alike).
+__host__ __device__ constexpr int fast_lines(int n, int real_bytes) {
+  return n == 512 ? 16 : (real_bytes == 4 ? 16 : 8);
+}
+
 template <int N, typename R> struct FastCfg {
-  static constexpr int L = N == 512 ? 8 : (sizeof(R) == 4 ? 16 : 8);
+  static constexpr int L = fast_lines(N, (int)sizeof(R));
   static constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
   static constexpr int P1 = L * N1, P2 = L * N2;
   static constexpr bool POW2 = (N & (N - 1)) == 0 && N <= 256;
@@ -93,7 +103,7 @@ template <int N, typename R> __host__ __device__ constexpr size_t fast_tables_by
 // the same at run time (host): the shell histogram of a diagnostic x sweep lives
 // in the tables region, so it holds at most this many bytes of bins
 inline size_t fast_tables_bytes_rt(int n, int real_bytes) {
-  const int L = n == 512 ? 8 : (real_bytes == 4 ? 16 : 8);
+  const int L = fast_lines(n, real_bytes);
   return (((size_t)(n + L) * (16 + 8) + (size_t)(n + 3 * L) * real_bytes) + 15) / 16 * 16;
 }
 
@@ -741,8 +751,10 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
 // compiler's choice.  Measured for complex64 at n = 128, 256: the plain FFT
 // sweeps are memory-bound and want 1024 threads per SM (64 registers at
 // T = 256); the fused modes keep 768 (85 registers) for their extra live state.
-// At n = 512 (32-point phase, up to 214 registers unbounded) 768 / 512 threads
-// per SM: 240 -> 291 steps/s at 512^3 despite a few hundred bytes of spills.
+// At n = 512 (32-point phase, up to 214 registers unbounded; 512-thread
+// blocks) one block per SM: plain sweeps 95 registers, fused ones 128 with a
+// few hundred bytes of spills in Z21/Z2 (bounds measured 240 -> 291 steps/s at
+// 512^3 with 8-line tiles).
 // The diagnostic z sweep (FP64 potential per point) keeps 512 threads per SM.
 template <int N, typename R, int MODE> struct FastBounds {
   static constexpr int value = (sizeof(R) == 4 && (N == 128 || N == 256))

@@ -989,7 +989,7 @@ int finish_diag(gpe_plan* p, int na, int nb, bool hist, std::vector<double>& hos
 // Tile counts of the diagnostic z and x sweeps (the partials to finish).
 void diag_tiles(const gpe_plan* p, bool fast, int& na, int& nb) {
   if (fast) {
-    const int lt = p->n == 512 ? 8 : (p->dtype == GPE_C64 ? 16 : 8);
+    const int lt = fast_lines(p->n, (int)p->csize / 2);
     na = p->n * p->n / lt;
     nb = p->n * (p->n / lt);
   } else {
