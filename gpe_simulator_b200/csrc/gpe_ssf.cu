@@ -502,7 +502,7 @@ const CUtensorMap* tma_maps(gpe_plan* p, const void* base, int fax) {
   const cuuint64_t n = (cuuint64_t)p->n;
   const cuuint64_t dims[3] = {n, n, n};
   const cuuint64_t strides[2] = {n * 8, n * n * 8};
-  const cuuint32_t lt = (cuuint32_t)FastCfg<128, float>::L;
+  const cuuint32_t lt = (cuuint32_t)fast_lines(p->n, 4);
   const cuuint32_t boxes[2][3] = {{lt, (cuuint32_t)n, 1}, {lt, 1, (cuuint32_t)n}};
   const cuuint32_t estr[3] = {1, 1, 1};
   gpe_plan::TmaMaps& c = p->tma_cache[p->tma_next];

@@ -207,7 +207,7 @@ __device__ __forceinline__ void tma_plain_body(const Phys& ph, const Sweep& sw, 
 }
 
 template <int N, int AX>
-__global__ void __launch_bounds__(FastCfg<N, float>::T, 3)
+__global__ void __launch_bounds__(FastCfg<N, float>::T, FastCfg<N, float>::T >= 512 ? 1 : 3)
     k_tma_plain(Phys ph, Sweep sw, FastOps op, const __grid_constant__ CUtensorMap map) {
   tma_plain_body<N, AX>(ph, sw, op, &map);
 }
