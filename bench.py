@@ -187,7 +187,8 @@ def ours(args, world, rank, local):
     beam = beam_in_reference_units(BEAM["amp"], BEAM["width"], BEAM["radius"], BEAM["omega"],
                                    BEAM["ramp_steps"] * DT)
     plan = Plan(N_GRID, x, k, dtype=torch.complex64, kind="real", beta=2 * G, dt=DT / 2,
-                static_expr=TRAP_REF, beam=beam, tma=args.path == "tma", fuse_planes=args.path == "plane")
+                static_expr=TRAP_REF, beam=beam, path=args.path)
+    args.path = plan.path   # "auto" resolved
     prep = Plan(N_GRID, x, k, dtype=torch.complex64, kind="imaginary", beta=2 * G, dt=DT,
                 static_expr=TRAP_REF)
     host0 = initial_state(x, seed=rank).astype(np.complex64)
@@ -486,9 +487,10 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 512^3 leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
-    ap.add_argument("--path", choices=("default", "tma", "plane"), default="default",
+    ap.add_argument("--path", choices=("default", "tma", "plane", "auto"), default="default",
                     help="sweep path of the main leg: default, tma (y/x pencils staged by TMA), "
-                         "plane (y/z sweeps fused per x-plane); identical results")
+                         "plane (y/z sweeps fused per x-plane), auto (timed once per device and "
+                         "cached); identical results")
     ap.add_argument("--serve-requests", type=int, default=120)
     ap.add_argument("--serve-rate", type=float, default=50.0)
     args = ap.parse_args()

@@ -48,7 +48,8 @@ def _dptr(values):
 class Plan:
     def __init__(self, n, x_array, k_array, *, dtype, kind, beta, dt, kinetic_coeff=1.0,
                  static_expr="0", dynamic_expr="0", k_cut=None, beam=None, nk_bins=0,
-                 local_fp64=None, generic_only=False, fuse_planes=False, exact_local=False, tma=False):
+                 local_fp64=None, generic_only=False, fuse_planes=False, exact_local=False, tma=False,
+                 path=None):
         if not torch.cuda.is_available():
             raise RuntimeError("gpe_simulator_b200 needs a CUDA device (sm_100a)")
         self.lib = _lib.load()
@@ -100,7 +101,17 @@ class Plan:
             local_fp64 = False
         d.local_fp64 = 1 if local_fp64 else 0
         # sweep path: 0 fastest, 1 generic only, 3 y/z sweeps fused per x-plane (complex64 n = 128, 256),
-        # 4 fastest with the y/x pencils staged by TMA (complex64 n = 128, 256; identical results)
+        # 4 fastest with the y/x pencils staged by TMA (complex64 n = 128, 256; identical results).
+        # ``path`` names it instead: "default", "tma", "plane", or "auto" (timed once per device,
+        # size, dtype and kind, then cached; see tune.py)
+        if path is not None:
+            if path == "auto":
+                from .tune import choose_path
+                path = choose_path(self.n, x, k, dtype, kind)
+            if path not in ("default", "tma", "plane"):
+                raise ValueError("path must be 'default', 'tma', 'plane' or 'auto'")
+            tma, fuse_planes = path == "tma", path == "plane"
+        self.path = "plane" if fuse_planes else ("tma" if tma else "default")
         d.generic_only = 1 if generic_only else (3 if fuse_planes else (4 if tma else 0))
         # exact local sub-flows: an accuracy mode that departs from the reference on purpose
         d.exact_local = 1 if exact_local else 0

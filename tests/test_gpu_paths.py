@@ -161,6 +161,28 @@ def test_tma_staged_sweeps_equal_plain_loads_bitwise(cuda, n, kind):
     assert staged.status() == 0 and plain.status() == 0
 
 
+def test_auto_path_is_timed_cached_and_bit_identical(cuda, tmp_path, monkeypatch):
+    """``Plan(path="auto")`` times the three complex64 sweep paths at 128^3 once,
+    caches the fastest, and computes the same bits as the default path."""
+    import json
+    from gpe_simulator_b200 import Beam, tune
+    monkeypatch.setenv("GPE_TUNE_CACHE", str(tmp_path / "paths.json"))
+    kw = dict(beta=800.0, dt=4e-4, static_expr=cases.TRAP, beam=Beam(20.0, 0.5, 2.0, 1.0, 0.004))
+    auto, x = make(128, 12.0, "real", torch.complex64, False, path="auto", **kw)
+    plain, _ = make(128, 12.0, "real", torch.complex64, False, **kw)
+    assert auto.path in tune.CANDIDATES and plain.path == "default"
+    cache = json.loads((tmp_path / "paths.json").read_text())
+    (entry,) = cache.values()
+    assert entry["path"] == auto.path
+    assert all(v > 0 for v in entry["ms_per_step"].values())
+    assert entry["ms_per_step"][auto.path] == min(entry["ms_per_step"].values())
+    a = torch.from_numpy(ssf.noisy_gaussian(x, seed=5)).to(torch.complex64).cuda()
+    b = a.clone()
+    auto.step(a, 6, 0)
+    plain.step(b, 6, 0)
+    assert torch.equal(a, b)
+
+
 @pytest.mark.parametrize("kind", ["imaginary", "real"])
 def test_fast_512_matches_generic(cuda, kind):
     """512^3 complex64 (the largest single solve): register-resident sweeps vs

@@ -178,3 +178,40 @@ def test_plan_create_rejects_bad_descriptors_without_a_gpu():
     d.static_g, d.static_g_len = bad, 3
     assert lib.gpe_plan_create(ctypes.byref(d), ctypes.byref(h)) == _lib.GPE_ERR_ARG
     assert "program" in _lib.last_error()
+
+
+def test_path_tuner_picks_and_caches_the_fastest_candidate(tmp_path, monkeypatch):
+    """``Plan(path="auto")``'s choice: every candidate timed once per (device, n,
+    dtype, kind), the fastest kept in the JSON cache; no timing on a cache hit or
+    where only one path exists."""
+    import json
+    import torch
+    from gpe_simulator_b200 import tune
+    monkeypatch.setenv("GPE_TUNE_CACHE", str(tmp_path / "paths.json"))
+    x = np.linspace(-6, 6, 128, endpoint=False)
+    k = 2 * np.pi * np.fft.fftfreq(128, 12 / 128)
+    calls = []
+    times = {"default": 0.30, "tma": 0.31, "plane": 0.29}
+
+    def timer(p):
+        calls.append(p)
+        return times[p]
+
+    def choose(n=128, dtype=torch.complex64, kind="real", dev="gpu-a"):
+        return tune.choose_path(n, x, k, dtype, kind, device_name=dev, timer=timer)
+
+    assert choose() == "plane"
+    assert sorted(calls) == sorted(tune.CANDIDATES)
+    calls.clear()
+    assert choose() == "plane" and calls == []                     # cached
+    assert choose(kind="imaginary") == "plane" and len(calls) == 3   # keyed by kind
+    calls.clear()
+    times["plane"] = 0.5
+    assert choose(n=256) == "default" and len(calls) == 3           # keyed by size
+    assert choose(dev="gpu-b") == "default"                          # keyed by device
+    calls.clear()
+    assert choose(n=64) == "default" and calls == []                # one path only
+    assert choose(dtype=torch.complex128) == "default" and calls == []
+    cache = json.loads((tmp_path / "paths.json").read_text())
+    entry = cache["gpu-a|n=128|complex64|real"]
+    assert entry["path"] == "plane" and set(entry["ms_per_step"]) == set(tune.CANDIDATES)
