@@ -53,6 +53,16 @@ PATH_KERNELS = {"tma": {"y": ("k_tma_plain<256, 1> (TMA-staged y sweep, 2 per st
                 "plane": {"z": ("k_plane<256, float, 3> (inverse y, Z21, forward y per x-plane)", "plane")}}
 
 
+def workload_config(world, path="default"):
+    """The ``config`` of both arms' lines (the sweep path only when not the default)."""
+    cfg = {"workload": WORKLOAD, "grid": N_GRID, "psi_bytes": N_GRID ** 3 * 8,
+           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+           "l2": "inputs larger than L2 (128 MiB psi vs 126 MB L2), no flush"}
+    if path != "default":
+        cfg["sweep_path"] = path
+    return cfg
+
+
 def measured_peak():
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
@@ -295,10 +305,7 @@ def ours(args, world, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
         "data": "synthetic (seeded noisy Gaussian relaxed 50 imaginary steps)",
-        "config": {"workload": WORKLOAD, "grid": N_GRID, "psi_bytes": nbytes,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "sweep_path": args.path,
-                   "l2": "inputs larger than L2 (128 MiB psi vs 126 MB L2), no flush"},
+        "config": workload_config(world, args.path),
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
@@ -469,7 +476,7 @@ def reference(args, world, rank):
     return {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "grid": N_GRID},
+            "data": "synthetic", "config": workload_config(world),
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
