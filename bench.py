@@ -10,7 +10,10 @@ Gaussian beam A = 10, w = 0.5, R = 2, angular rate ramped 0 -> 0.5 over the firs
 an exact reparametrisation.  Inputs are synthetic (seeded noisy Gaussian relaxed
 for 50 imaginary-time steps); psi is 128 MiB, larger than the 126 MB L2.
 
-On one GPU the line also carries ``batched`` (64 imaginary-time solves of mixed
+On one GPU the line also carries ``plain_floor`` (the reference's step sequence
+with cuFFT through torch.fft and byte-equivalent elementwise kernels: a floor on
+the reference's step time on the same GPU, since its CuPy code cannot run here),
+``stir512`` (the same physics at 512^3), ``batched`` (64 imaginary-time solves of mixed
 grid sizes as one running batch vs one at a time: solves/s) and ``serving`` (a
 seeded request stream through the continuous-batching server vs the plain path:
 solves/s, p50/p99 latency, results identical) -- the other two parts of the
@@ -326,6 +329,8 @@ def ours(args, world, rank, local):
     }
     if world == 1 and rank == 0 and not args.no_cpu:
         result["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+    if world == 1 and not args.no_plain:
+        result["plain_floor"] = plain_floor_leg()
     if world == 1 and not args.no_large:
         result["stir512"] = large_leg()
     if world == 1 and not args.no_batch:
@@ -366,6 +371,53 @@ def large_leg(steps=100, warmup=5):
     return {"grid": n, "steps": steps, "steps_per_s": 1e3 / ms, "ms_per_step": ms,
             "step_roofline_frac": 6 * 8 * m / (ms / 1e3) / 1e9 / peak,
             "data": "Gaussian trap state, synthetic"}
+
+
+def plain_floor_leg(steps=50, warmup=5):
+    """Floor of the reference's own step time on this GPU (CuPy is not installed,
+    so its code cannot run here): the reference's sequence per step -- half-step
+    kernel, fftn, kinetic kernel, ifftn, half-step kernel -- with cuFFT through
+    torch.fft (out of place, as cp.fft) and each elementwise RawKernel replaced
+    by one torch kernel moving the same bytes (half-step: psi and staticV read,
+    psi written, 48 B/point in complex128; kinetic: psi_k read and written) but
+    doing less arithmetic.  complex128 as the reference ships, complex64 for
+    comparison; the reference's steps cannot be faster than these."""
+    import torch
+    out = {}
+    n = N_GRID
+    for name, dtype in (("c128", torch.complex128), ("c64", torch.complex64)):
+        g = torch.Generator(device="cuda").manual_seed(0)
+        real = torch.float64 if dtype == torch.complex128 else torch.float32
+        psi = torch.randn((n, n, n), dtype=dtype, device="cuda", generator=g)
+        # unit-modulus factors keep repeated steps finite and normal
+        ang = torch.randn((n, n, n), dtype=real, device="cuda", generator=g)
+        pot = torch.polar(torch.ones_like(ang), ang)
+        del ang
+
+        def step(psi):
+            torch.mul(psi, pot, out=psi)
+            f = torch.fft.fftn(psi)
+            f.mul_(complex(0.6, 0.8))
+            psi = torch.fft.ifftn(f)
+            torch.mul(psi, pot, out=psi)
+            return psi
+
+        for _ in range(warmup):
+            psi = step(psi)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            psi = step(psi)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms_per_step": ms, "steps_per_s": 1e3 / ms}
+        del psi, pot
+        torch.cuda.empty_cache()
+    out["note"] = ("reference step sequence at 256^3: cuFFT via torch.fft + byte-equivalent torch "
+                   "elementwise kernels in place of its RawKernels; a floor on its step time")
+    return out
 
 
 def batched_leg():
@@ -493,6 +545,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 512^3 leg")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the floor of the reference's step sequence (cuFFT via torch.fft)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--path", choices=("default", "tma", "plane", "auto"), default="default",
                     help="sweep path of the main leg: default, tma (y/x pencils staged by TMA), "
