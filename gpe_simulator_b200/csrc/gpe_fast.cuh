@@ -525,7 +525,7 @@ __device__ __forceinline__ void diag_k_all(const typename Cx<R>::T (&v)[EPT], co
       int i, j, k;
       tl.coords(l, m, i, j, k);
       const typename Cx<R>::T x = v[s * VALS + a];
-      const double kk = ph.k[i] * ph.k[i] + ph.k[j] * ph.k[j] + ph.k[k] * ph.k[k];
+      const double kk = kk_ref(ph.k[i], ph.k[j], ph.k[k]);
       const double w = (double)x.x * x.x + (double)x.y * x.y;
       e = fma(kk, w, e);
       if (cx.hist) {

@@ -285,6 +285,13 @@ __device__ __forceinline__ typename Cx<R>::T kinetic(const Phys& ph, typename Cx
   return mk((R)(vx * f.x - vy * f.y), (R)(vx * f.y + vy * f.x));
 }
 
+// |k|^2 = kx^2 + ky^2 + kz^2 rounded as NumPy evaluates it (each product and sum
+// rounded, left to right, no fused multiply-add), so shell indices at exact
+// boundaries agree with the reference's nk_extraction.
+__device__ __forceinline__ double kk_ref(double kx, double ky, double kz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), __dmul_rn(kz, kz));
+}
+
 // Per-point pointwise stage.
 template <typename R>
 struct PwCtx {
@@ -322,7 +329,7 @@ __device__ __forceinline__ typename Cx<R>::T pointwise(const Phys& ph, unsigned 
   if (ops & PW_NORM) cx.acc[0].add((double)v.x * v.x + (double)v.y * v.y);
   if (ops & PW_DIAG_K) {
     // reference gpe/helper.py:116-121 and gpe/nk_extraction.py:5-13
-    const double kk = ph.k[i] * ph.k[i] + ph.k[j] * ph.k[j] + ph.k[k] * ph.k[k];
+    const double kk = kk_ref(ph.k[i], ph.k[j], ph.k[k]);
     const double w = (double)v.x * v.x + (double)v.y * v.y;
     cx.acc[3].add(kk * w);
     int sh = (int)floor(sqrt(kk) / cx.shell_w + 0.5);

@@ -179,6 +179,50 @@ __global__ void k_finish_diag(const double* pa, int na, const double* pb, int nb
     for (int v = 0; v < 4; ++v) out[v] = a[v].value();
 }
 
+// k-space sums of a spectrum passed in by the caller (no transform): sum k^2 |f|^2
+// (the reference's get_E, gpe/helper.py:135-140) into partial[block * 4 + 3] and,
+// with `hist`, the block's shell histogram of |f|^2 (gpe/nk_extraction.py:5-21)
+// into hist[block][nbins].  Each warp walks whole rows (x, y) with its lanes
+// along z, so the row's k_x^2 + k_y^2 and indices are computed once per row.
+template <typename C>
+__global__ void __launch_bounds__(256) k_kspace(const C* __restrict__ f, int n, const double* __restrict__ k,
+                                                double* __restrict__ partial, double* __restrict__ hist,
+                                                int nbins, double shell_w) {
+  extern __shared__ double sh_hist[];
+  __shared__ Acc red[32];
+  if (hist) {
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) sh_hist[b] = 0.0;
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  double e = 0.0;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n * n; r += warps) {
+    const int i = r / n, j = r - i * n;
+    const double kx = k[i], ky = k[j];
+    const C* row = f + (long long)r * n;
+    for (int z = lane; z < n; z += 32) {
+      const double kk = kk_ref(kx, ky, k[z]);
+      const C v = row[z];
+      const double w = (double)v.x * v.x + (double)v.y * v.y;
+      e = fma(kk, w, e);
+      if (hist) {
+        int sh = (int)floor(sqrt(kk) / shell_w + 0.5);
+        sh = min(sh, nbins - 1);
+        atomicAdd(sh_hist + sh, w);
+      }
+    }
+  }
+  Acc a[1];
+  a[0].add(e);
+  block_merge<1>(a, red);
+  if (threadIdx.x == 0) partial[(long long)blockIdx.x * 4 + 3] = a[0].value();
+  if (hist) {
+    __syncthreads();
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) hist[(long long)blockIdx.x * nbins + b] = sh_hist[b];
+  }
+}
+
 // Shell histograms: block `bin` sums that bin over the nb per-tile histograms
 // (threads stride over the tiles with compensation, merged in a fixed order)
 // into out[4 + bin].
@@ -964,13 +1008,29 @@ int fft3d(gpe_plan* p, const void* in, void* out, bool inverse, cudaStream_t st)
 }
 
 // k-space reductions of a spectrum `f` (no FFT): partial area B + histogram.
-int kspace_reduce(gpe_plan* p, const void* f, cudaStream_t st) {
+// k-space reductions of a spectrum `f` (no FFT): per-block sums of k^2 |f|^2
+// (+ shell histograms) into partial area B; `nb` = the blocks to finish.
+int kspace_reduce(gpe_plan* p, const void* f, bool hist, int& nb, cudaStream_t st) {
   TRY(ensure_hist(p));
-  Sweep s = mk_sweep(f, nullptr);
-  s.post = PW_DIAG_K;
-  s.partial = p->d_partial + 4 * (size_t)p->max_tiles;
-  s.hist = p->d_hist;
-  return sweep(p, AX_X, s, st);
+  // at most max_tiles blocks (the partial and histogram areas), 4 per SM
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const size_t smem = hist ? (size_t)p->nbins * sizeof(double) : 0;
+  if (smem > 48 * 1024) return fail(GPE_ERR_UNSUPPORTED, "too many n(k) bins for the shared histogram");
+  nb = std::max(1, std::min(p->max_tiles, std::min(4 * sms, (p->n * p->n + 7) / 8)));
+  double* part = p->d_partial + 4 * (size_t)p->max_tiles;
+  double* h = hist ? p->d_hist : nullptr;
+  if (p->dtype == GPE_C64)
+    k_kspace<float2><<<nb, 256, smem, st>>>((const float2*)f, p->n, p->d_k, part, h, p->nbins, p->shell_w);
+  else
+    k_kspace<double2><<<nb, 256, smem, st>>>((const double2*)f, p->n, p->d_k, part, h, p->nbins, p->shell_w);
+  CU(cudaGetLastError());
+  ++p->launches;
+  return GPE_OK;
 }
 
 int finish_diag(gpe_plan* p, int na, int nb, bool hist, std::vector<double>& host, cudaStream_t st) {
@@ -1279,9 +1339,10 @@ int gpe_norm(gpe_plan* p, const void* psi, double* norm, void* stream) {
 int gpe_kinetic_energy(gpe_plan* p, const void* psi_k, double* e_kin, void* stream) {
   if (!p || !psi_k || !e_kin) return fail(GPE_ERR_ARG, "null argument");
   cudaStream_t st = (cudaStream_t)stream;
-  TRY(kspace_reduce(p, psi_k, st));
+  int nb = 0;
+  TRY(kspace_reduce(p, psi_k, false, nb, st));
   std::vector<double> h;
-  TRY(finish_diag(p, 0, tiles_of(p, AX_X), false, h, st));
+  TRY(finish_diag(p, 0, nb, false, h, st));
   *e_kin = h[3] * p->ph.dx3 * p->ph.inv_m;
   return GPE_OK;
 }
@@ -1289,9 +1350,10 @@ int gpe_kinetic_energy(gpe_plan* p, const void* psi_k, double* e_kin, void* stre
 int gpe_nk_extraction(gpe_plan* p, const void* psi_k, double* occupation, long long* counts, void* stream) {
   if (!p || !psi_k) return fail(GPE_ERR_ARG, "null argument");
   cudaStream_t st = (cudaStream_t)stream;
-  TRY(kspace_reduce(p, psi_k, st));
+  int nb = 0;
+  TRY(kspace_reduce(p, psi_k, true, nb, st));
   std::vector<double> h;
-  TRY(finish_diag(p, 0, tiles_of(p, AX_X), true, h, st));
+  TRY(finish_diag(p, 0, nb, true, h, st));
   const double f = p->ph.dx3 * p->ph.inv_m;
   if (occupation)
     for (int b = 0; b < p->nbins; ++b) occupation[b] = h[4 + b] * f;
