@@ -46,6 +46,23 @@ def _dptr(values):
 
 
 class Plan:
+    """One propagator configuration (``gpe_plan_create``).
+
+    ``n``, ``x_array``, ``k_array``: grid (the reference's ``stage.N_grids``,
+    ``x_array``, ``k_array``); ``dtype``: ``torch.complex64`` or ``complex128``;
+    ``kind``: ``"imaginary"`` or ``"real"``; ``beta``, ``dt``, ``kinetic_coeff``:
+    the step's coefficients (1.0 = the reference's ``exp(-i k^2 dt)``);
+    ``static_expr`` / ``dynamic_expr``: potentials in the reference's expression
+    grammar; ``k_cut``: momentum cutoff (real time); ``beam``: built-in stirring
+    beam; ``nk_bins``: 0 = the reference's shell binning, else uniform bins.
+    Options that keep results identical: ``path`` (``"default"``, ``"tma"``,
+    ``"plane"`` or ``"auto"``: the sweep path, see ``tune.py``; ``tma`` and
+    ``fuse_planes`` are the older switches for two of them) and
+    ``generic_only`` (mixed-radix sweeps only).  Options that change results on
+    purpose: ``local_fp64`` (complex64 local factor in FP64) and ``exact_local``
+    (exact local sub-flows).
+    """
+
     def __init__(self, n, x_array, k_array, *, dtype, kind, beta, dt, kinetic_coeff=1.0,
                  static_expr="0", dynamic_expr="0", k_cut=None, beam=None, nk_bins=0,
                  local_fp64=None, generic_only=False, fuse_planes=False, exact_local=False, tma=False,
