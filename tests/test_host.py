@@ -215,3 +215,27 @@ def test_path_tuner_picks_and_caches_the_fastest_candidate(tmp_path, monkeypatch
     cache = json.loads((tmp_path / "paths.json").read_text())
     entry = cache["gpu-a|n=128|complex64|real"]
     assert entry["path"] == "plane" and set(entry["ms_per_step"]) == set(tune.CANDIDATES)
+
+
+def test_ctypes_signatures_match_the_header_prototypes():
+    """Every prototype in include/gpe_ssf.h and its ctypes argtypes agree in the
+    number of parameters and in each scalar type (pointers as any pointer type)."""
+    from gpe_simulator_b200 import _lib
+    text = Path(HEADER).read_text()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    protos = dict(re.findall(r"^\s*(?:int|const char\*)\s+(gpe_\w+)\s*\(([^)]*)\)\s*;", text, re.M))
+    assert set(protos) == set(declared_functions())
+    scalar = {"double": ctypes.c_double, "int": ctypes.c_int, "long long": ctypes.c_longlong,
+              "unsigned": ctypes.c_uint, "size_t": ctypes.c_size_t}
+    pointer_like = (ctypes.c_void_p, ctypes.c_char_p)
+    for name, params in protos.items():
+        params = " ".join(params.split())
+        parts = [] if params in ("", "void") else [p.strip() for p in params.split(",")]
+        argtypes = _lib.SIGNATURES[name]
+        assert len(parts) == len(argtypes), (name, parts, argtypes)
+        for p, t in zip(parts, argtypes):
+            if "*" in p:
+                assert t in pointer_like or issubclass(t, ctypes._Pointer), (name, p, t)
+            else:
+                base = re.sub(r"^const\s+", "", p).rsplit(" ", 1)[0]
+                assert t is scalar[base], (name, p, t)
