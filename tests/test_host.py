@@ -254,3 +254,23 @@ def test_integration_guide_descriptor_matches_the_library():
     assert ctypes.sizeof(Doc) == ctypes.sizeof(_lib.Desc)
     for (f, _), (g, _) in zip(Doc._fields_, _lib.Desc._fields_):
         assert getattr(Doc, f).offset == getattr(_lib.Desc, g).offset, f
+
+
+def test_python_constants_match_the_header():
+    """Status codes, dtype/kind/potential kinds, bytecode opcodes and projection
+    bits as the Python layer spells them equal the header's #defines."""
+    from gpe_simulator_b200 import _lib, expressions
+    from gpe_simulator_b200.plan import Plan
+    defs = {k: int(v) for k, v in re.findall(r"^#define\s+(GPE_\w+)\s+(\d+)u?\b", Path(HEADER).read_text(), re.M)}
+    for name in ("GPE_OK", "GPE_ERR_ARG", "GPE_ERR_UNSUPPORTED", "GPE_ERR_CUDA", "GPE_ERR_OOM",
+                 "GPE_ERR_NONFINITE", "GPE_ERR_TIMEOUT"):
+        assert getattr(_lib, name) == defs[name], name
+    for py, c in (("C64", "GPE_C64"), ("C128", "GPE_C128"), ("IMAGINARY", "GPE_IMAGINARY"), ("REAL", "GPE_REAL"),
+                  ("V_NONE", "GPE_V_NONE"), ("V_REAL64", "GPE_V_REAL64"), ("V_CPLX128", "GPE_V_CPLX128")):
+        assert getattr(_lib, py) == defs[c], py
+    for op in ("CONST", "X", "Y", "Z", "T", "ADD", "SUB", "MUL", "DIV", "POW", "NEG"):
+        assert getattr(expressions, "OP_" + op) == defs["GPE_OP_" + op], op
+    for fn, code in expressions._FUNC_OP.items():
+        assert code == defs["GPE_OP_" + fn.upper()], fn
+    for i, name in enumerate(Plan.PROJECTIONS):
+        assert defs["GPE_PROJ_" + name.upper()] == 1 << i, name
