@@ -274,3 +274,33 @@ def test_python_constants_match_the_header():
         assert code == defs["GPE_OP_" + fn.upper()], fn
     for i, name in enumerate(Plan.PROJECTIONS):
         assert defs["GPE_PROJ_" + name.upper()] == 1 << i, name
+
+
+def test_product_code_does_not_reach_the_oracle():
+    """The package never imports ``oracle``; bench.py imports it only inside its
+    CPU legs (``cpu_baseline``, whose caller ``reference`` is the CPU arm)."""
+    import ast
+    root = Path(__file__).resolve().parents[1]
+
+    def oracle_imports(path):
+        tree = ast.parse(path.read_text())
+        found = []
+
+        def visit(node, func):
+            for child in ast.iter_child_nodes(node):
+                f = child.name if isinstance(child, (ast.FunctionDef, ast.AsyncFunctionDef)) else func
+                mods = []
+                if isinstance(child, ast.Import):
+                    mods = [a.name for a in child.names]
+                elif isinstance(child, ast.ImportFrom):
+                    mods = [child.module or ""]
+                if any(m == "oracle" or m.startswith("oracle.") for m in mods):
+                    found.append(f)
+                visit(child, f)
+
+        visit(tree, None)
+        return found
+
+    for src in sorted((root / "gpe_simulator_b200").rglob("*.py")):
+        assert oracle_imports(src) == [], src
+    assert set(oracle_imports(root / "bench.py")) <= {"cpu_baseline"}
