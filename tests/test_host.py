@@ -304,3 +304,20 @@ def test_product_code_does_not_reach_the_oracle():
     for src in sorted((root / "gpe_simulator_b200").rglob("*.py")):
         assert oracle_imports(src) == [], src
     assert set(oracle_imports(root / "bench.py")) <= {"cpu_baseline"}
+
+
+def test_missing_library_and_missing_gpu_fail_loudly(tmp_path, monkeypatch):
+    """No CPU fallback: without the built library the loader raises, and a plan
+    refuses to exist without a CUDA device (this container has none)."""
+    import torch
+    from gpe_simulator_b200 import _lib
+    from gpe_simulator_b200.plan import Plan
+    monkeypatch.setattr(_lib, "_lib", None)
+    monkeypatch.setattr(_lib, "LIB_PATH", tmp_path / "libgpe_ssf.so")
+    with pytest.raises(RuntimeError, match="not built"):
+        _lib.load()
+    if not torch.cuda.is_available():
+        x = np.linspace(-4, 4, 16, endpoint=False)
+        with pytest.raises(RuntimeError, match="CUDA device"):
+            Plan(16, x, 2 * np.pi * np.fft.fftfreq(16, 0.5), dtype=torch.complex64, kind="imaginary",
+                 beta=1.0, dt=1e-3)
