@@ -163,8 +163,8 @@ __global__ void k_build_static(int n, const double* x, const double* prog, int l
   }
 }
 
-// Sum per-block diagnostic partials in a fixed order.
-// out[0..3] = sums of pa columns 0..2 and pb column 3; out[4 + b] = histogram bin b.
+// Sum per-block diagnostic partials in a fixed order: out[0..3] = sums of pa
+// columns 0..2 and pb column 3 (the shell bins out[4 + b] come from k_finish_hist).
 __global__ void k_finish_diag(const double* pa, int na, const double* pb, int nb, double* out) {
   __shared__ Acc sh[32 * 4];
   Acc a[4];
@@ -535,8 +535,9 @@ EncodeTiledFn encode_tiled() {
 }
 
 // Tensor maps of the n^3 complex64 array at `base` (8-byte elements, dims z, y,
-// x innermost first): y tiles are boxes {16, n, 1}, x tiles {16, 1, n}.  Null
-// when the array cannot be staged (base not 16-byte aligned, encoder missing).
+// x innermost first): y tiles are boxes {L, n, 1}, x tiles {L, 1, n}, L the
+// sweeps' lines per tile.  Null when the array cannot be staged (base not
+// 16-byte aligned, encoder missing).
 const CUtensorMap* tma_maps(gpe_plan* p, const void* base, int fax) {
   const int which = fax == FY ? 0 : 1;
   for (auto& c : p->tma_cache)
