@@ -18,14 +18,24 @@
 //    contents: the completion ticket and status word are cleared at the start
 //    of every call, and calls whose work overlaps on the GPU (different streams,
 //    no ordering between them) race on it -- serialise them;
-//  * the first call on each device looks up the array's device address with
-//    cudaGetSymbolAddress (module set-up); make that first call before any
-//    stream capture.
+//  * set-up happens on the first call in each CUDA context (normally one per
+//    device): it looks up the array's device address with cudaGetSymbolAddress
+//    and loads this file's four kernels, so that no later call loads code (with
+//    CUDA's lazy module loading a first launch would otherwise load it, taking
+//    device memory); make that first call before any stream capture.  The
+//    address is cached per context id, so a context torn down and created again
+//    (cudaDeviceReset) gets a fresh look-up instead of a stale address;
+//  * every call synchronises `stream`: it reads the status word back and
+//    returns GPE_ERR_NONFINITE, with psi left unchanged, when N is zero, NaN or
+//    infinite.
 #include "../../include/gpe_ssf.h"
 #include "gpe_kernels.cuh"
 
+#include <cuda.h>
+
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 using namespace gpe;
@@ -48,28 +58,35 @@ static_assert(8 * GPE_NOALLOC_BLOCKS + 40 <= SCRATCH_BYTES, "scratch too small")
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[SCRATCH_BYTES];
 
-constexpr int MAX_DEVICES = 64;
-void* g_scratch_ptr[MAX_DEVICES] = {nullptr};
-
 int fail_na(int code, const std::string& msg) {
   gpe::set_last_error(msg);
   return code;
 }
 
-// Device address of the scratch array on the current device (set-up on first use).
-int scratch_address(void** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return fail_na(GPE_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= MAX_DEVICES) return fail_na(GPE_ERR_UNSUPPORTED, "device index out of range");
-  if (!g_scratch_ptr[dev]) {
-    void* ptr = nullptr;
-    e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess)
-      return fail_na(GPE_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_scratch_ptr[dev] = ptr;
+// Context id of the calling thread's current context (cuCtxGetCurrent +
+// cuCtxGetId from the driver, reached through the runtime's entry-point query,
+// so the library needs no link-time dependency on libcuda).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+int current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return fail_na(GPE_ERR_CUDA, "cuCtxGetCurrent is not available from the driver");
+    get_current = (CtxGetCurrentFn)f;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return fail_na(GPE_ERR_CUDA, "cuCtxGetId is not available from the driver");
+    get_id = (CtxGetIdFn)f;
   }
-  *out = g_scratch_ptr[dev];
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return fail_na(GPE_ERR_CUDA, "no current CUDA context");
+  if (get_id(ctx, id) != CUDA_SUCCESS) return fail_na(GPE_ERR_CUDA, "cuCtxGetId failed");
   return GPE_OK;
 }
 
@@ -113,11 +130,14 @@ k_norm_noalloc(const typename Cx<R>::T* __restrict__ psi, long long m, double dx
   }
 }
 
-// psi /= sqrt(N) (reference gpe/helper.py:93), reading sqrt(N) from the scratch.
+// psi /= sqrt(N) (reference gpe/helper.py:93), reading sqrt(N) from the scratch;
+// nothing is written when the norm kernel flagged N as zero or non-finite.
 template <typename R>
 __global__ void __launch_bounds__(GPE_NOALLOC_THREADS)
 k_scale_noalloc(typename Cx<R>::T* __restrict__ psi, long long m, const unsigned char* scratch) {
   const double* scale = (const double*)scratch + GPE_NOALLOC_BLOCKS;
+  const int* status = (const int*)((const unsigned*)(scale + 4) + 1);
+  if (__ldcg(status) & ST_NONFINITE) return;   // zero or non-finite N: psi left as it is
   const double s = __ldcg(scale);
   const R inv = (R)__ldcg(scale + 1);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
@@ -127,6 +147,39 @@ k_scale_noalloc(typename Cx<R>::T* __restrict__ psi, long long m, const unsigned
     else { v.x *= inv; v.y *= inv; }
     psi[i] = v;
   }
+}
+
+// Scratch address per CUDA context (a context id is never reused in a process).
+constexpr int MAX_CONTEXTS = 64;
+struct ScratchSlot { unsigned long long ctx; void* ptr; };
+ScratchSlot g_slots[MAX_CONTEXTS] = {};
+int g_nslots = 0;
+std::mutex g_slots_mu;
+
+// Device address of the scratch array in the current context; the first call
+// in a context also loads this file's kernels (both precisions).
+int scratch_address(void** out) {
+  unsigned long long ctx = 0;
+  int rc = current_context_id(&ctx);
+  if (rc != GPE_OK) return rc;
+  std::lock_guard<std::mutex> lock(g_slots_mu);
+  for (int i = 0; i < g_nslots; ++i)
+    if (g_slots[i].ctx == ctx) { *out = g_slots[i].ptr; return GPE_OK; }
+  if (g_nslots == MAX_CONTEXTS) return fail_na(GPE_ERR_UNSUPPORTED, "too many CUDA contexts");
+  void* ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess) return fail_na(GPE_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  // load the kernels now (a lazily loaded module would load on first launch)
+  cudaFuncAttributes fa;
+  const void* fns[4] = {(const void*)k_norm_noalloc<float>, (const void*)k_scale_noalloc<float>,
+                        (const void*)k_norm_noalloc<double>, (const void*)k_scale_noalloc<double>};
+  for (const void* f : fns) {
+    e = cudaFuncGetAttributes(&fa, f);
+    if (e != cudaSuccess) return fail_na(GPE_ERR_CUDA, std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(e));
+  }
+  g_slots[g_nslots++] = ScratchSlot{ctx, ptr};
+  *out = ptr;
+  return GPE_OK;
 }
 
 }  // namespace
@@ -158,10 +211,14 @@ extern "C" int gpe_normalise_noalloc(void* psi, int n, int dtype, double dx, dou
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail_na(GPE_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
-  if (norm) {
-    e = cudaMemcpyAsync(norm, base + 8 * GPE_NOALLOC_BLOCKS + 16, sizeof(double), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return fail_na(GPE_ERR_CUDA, std::string("read back: ") + cudaGetErrorString(e));
-  }
+  // N, the spare slot, the ticket and the status word, read back in one copy
+  struct { double N, spare; unsigned ticket; int status; } back;
+  static_assert(sizeof(back) == 24, "read-back layout");
+  e = cudaMemcpyAsync(&back, base + 8 * GPE_NOALLOC_BLOCKS + 16, sizeof(back), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail_na(GPE_ERR_CUDA, std::string("read back: ") + cudaGetErrorString(e));
+  if (norm) *norm = back.N;
+  if (back.status & ST_NONFINITE)
+    return fail_na(GPE_ERR_NONFINITE, "gpe_normalise_noalloc: the norm is zero or not finite; psi is unchanged");
   return GPE_OK;
 }

@@ -21,7 +21,10 @@
 // holds the SMs until its last tile, ending the programmatic overlap with the
 // neighbouring sweeps.
 // Every wait on an mbarrier is bounded (GPE_TMA_WAIT_NS of global time); on
-// expiry the block records ST_TIMEOUT and all its threads leave together.
+// expiry the block records ST_TIMEOUT, issues no further copy, waits once more
+// (bounded) for the copies it has in flight, and all its threads leave together.
+// A copy that outlasts that second wait too can still land after the block has
+// left; the status word reports the timeout either way.
 #pragma once
 #include <cuda.h>
 #include "gpe_fast.cuh"
@@ -172,6 +175,13 @@ __device__ __forceinline__ void tma_plain_body(const Phys& ph, const Sweep& sw, 
     const bool done = mbar_wait_bounded(&bar[s], (unsigned)(it >> 1) & 1u);
     if (__syncthreads_or(!done)) {
       if (threadIdx.x == 0) atomicOr(sw.status, ST_TIMEOUT);
+      // Copies still in flight write into this block's shared memory, which the
+      // SM may hand to another block once this one exits: issue nothing more
+      // and wait once more (bounded) for the late copy of this stage and for
+      // the prefetch of the next tile into the other stage, if one was issued.
+      mbar_wait_bounded(&bar[s], (unsigned)(it >> 1) & 1u);
+      if (tile + stride < NT) mbar_wait_bounded(&bar[s ^ 1], (unsigned)((it + 1) >> 1) & 1u);
+      __syncthreads();
       return;
     }
     // registers in layout (N1 lanes, N2 values); the staged box is [m][l]

@@ -5,6 +5,7 @@ Drop-in counterparts of ``gpe/grids.py``, ``gpe/helper.py`` and
 ``libgpe_ssf.so`` through a cached utility plan per (grid, dtype, device).
 """
 
+from collections import OrderedDict
 import math
 
 import numpy as np
@@ -12,7 +13,11 @@ import torch
 
 from .plan import Plan
 
-_UTIL = {}
+# utility plans by (grid, dtype, device, shell binning), least recently used first;
+# the oldest is dropped once more than _UTIL_MAX are held (a plan frees its tables when
+# no caller holds it any more)
+_UTIL = OrderedDict()
+_UTIL_MAX = 16
 
 
 def get_grids(N_grids, simulation_range, device="cuda"):
@@ -22,8 +27,10 @@ def get_grids(N_grids, simulation_range, device="cuda"):
     return torch.from_numpy(x).to(device), torch.from_numpy(k).to(device)
 
 
-def utility_plan(psi, x_array, k_array=None):
-    """Plan without physics, for FFTs and reductions on ``psi``'s grid."""
+def utility_plan(psi, x_array, k_array=None, nbins=0):
+    """Plan without physics, for FFTs and reductions on ``psi``'s grid (``nbins``:
+    0 = the reference's shell binning, else that many uniform bins).  Plans are
+    cached, so repeated diagnostics on one grid create no new device tables."""
     n = psi.shape[0]
     xs = x_array.detach().cpu().numpy() if isinstance(x_array, torch.Tensor) else np.asarray(x_array)
     if k_array is None:
@@ -31,12 +38,16 @@ def utility_plan(psi, x_array, k_array=None):
         ks = 2 * np.pi * np.fft.fftfreq(n, L / n)
     else:
         ks = k_array.detach().cpu().numpy() if isinstance(k_array, torch.Tensor) else np.asarray(k_array)
-    key = (n, psi.dtype, psi.device.index, float(xs[0]), float(xs[1]), float(ks[1]))
+    key = (n, psi.dtype, psi.device.index, float(xs[0]), float(xs[1]), float(ks[1]), int(nbins or 0))
     plan = _UTIL.get(key)
     if plan is None:
         with torch.cuda.device(psi.device):
-            plan = Plan(n, xs, ks, dtype=psi.dtype, kind="imaginary", beta=0.0, dt=0.0)
+            plan = Plan(n, xs, ks, dtype=psi.dtype, kind="imaginary", beta=0.0, dt=0.0, nk_bins=int(nbins or 0))
         _UTIL[key] = plan
+        while len(_UTIL) > _UTIL_MAX:
+            _UTIL.popitem(last=False)
+    else:
+        _UTIL.move_to_end(key)
     return plan
 
 

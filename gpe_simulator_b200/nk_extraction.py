@@ -10,7 +10,6 @@ import math
 import numpy as np
 
 from .helper import utility_plan
-from .plan import Plan
 
 
 def shell_geometry(n, dk, nbins=None):
@@ -41,10 +40,6 @@ def nk_extraction(psi_k, x_array, k_array, slab_size=16, nbins=None):
     n = psi_k.shape[0]
     ks = k_array.detach().cpu().numpy()
     dk = abs(float(ks[1] - ks[0]))
-    if nbins:
-        xs = x_array.detach().cpu().numpy()
-        plan = Plan(n, xs, ks, dtype=psi_k.dtype, kind="imaginary", beta=0.0, dt=0.0, nk_bins=nbins)
-    else:
-        plan = utility_plan(psi_k, x_array, k_array)
+    plan = utility_plan(psi_k, x_array, k_array, nbins=nbins or 0)
     Nk, counts = plan.shells(psi_k)
     return assemble(Nk, counts, n, dk, nbins)

@@ -229,9 +229,10 @@ int  gpe_batch_launch_count(const gpe_batch* batch, long long* count);
  * The reduction scratch is a fixed 16 KiB file-scope device array per GPU (held
  * until the process exits).  Limit: n <= 1024 (2^30 points); larger grids are
  * rejected with GPE_ERR_UNSUPPORTED.  All calls on a device share that array, so
- * calls that overlap on the GPU race; the first call on each device looks up the
- * array's address and should come before any stream capture.  norm (nullable, host)
- * receives N and then the call synchronises `stream`. */
+ * calls that overlap on the GPU race.  The first call in each CUDA context looks up
+ * the array's address and loads the kernels of both precisions; make it before any
+ * stream capture.  Every call synchronises `stream`: norm (nullable, host) receives
+ * N, and a zero, NaN or infinite N returns GPE_ERR_NONFINITE with psi unchanged. */
 int  gpe_normalise_noalloc(void* psi, int n, int dtype, double dx, double* norm, void* stream);
 
 #ifdef __cplusplus

@@ -37,7 +37,15 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
+# This recipe reads the reference's sources where the build container mounts
+# them; GPE_REFERENCE points it elsewhere.  Nothing on the product path, in the
+# GPU tests or in the bench reads them.
 REFERENCE = Path(os.environ.get("GPE_REFERENCE", "/root/reference"))
+
+
+def available():
+    """True when the reference's sources are present for this recipe."""
+    return (REFERENCE / "gpe" / "make_propagator.py").exists()
 
 _COMPLEX_HEADER = r"""
 #pragma once

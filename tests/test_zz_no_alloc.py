@@ -68,20 +68,50 @@ def test_two_calls_match_plan_based_normalise(cuda, dtype, code, tol):
 
 
 def test_no_device_memory_is_allocated(cuda):
+    """After the first call in the context (which also loads both precisions'
+    kernels), calls of either precision take no device memory."""
     so, _lib = lib()
     n = 32
-    psi = torch.ones((n, n, n), dtype=torch.complex64, device="cuda")
-    # first call: module set-up on this device
-    assert so.gpe_normalise_noalloc(ctypes.c_void_p(psi.data_ptr()), n, 0, 0.5, None, stream()) == 0
+    psi64 = torch.ones((n, n, n), dtype=torch.complex64, device="cuda")
+    psi128 = torch.ones((n, n, n), dtype=torch.complex128, device="cuda")
+    torch.cuda.synchronize()
+    # first call: set-up in this context
+    assert so.gpe_normalise_noalloc(ctypes.c_void_p(psi64.data_ptr()), n, 0, 0.5, None, stream()) == 0
     torch.cuda.synchronize()
     free0, _ = torch.cuda.mem_get_info()
     for _ in range(3):
-        assert so.gpe_normalise_noalloc(ctypes.c_void_p(psi.data_ptr()), n, 0, 0.5, None, stream()) == 0
+        assert so.gpe_normalise_noalloc(ctypes.c_void_p(psi128.data_ptr()), n, 1, 0.5, None, stream()) == 0
+        assert so.gpe_normalise_noalloc(ctypes.c_void_p(psi64.data_ptr()), n, 0, 0.5, None, stream()) == 0
     torch.cuda.synchronize()
     free1, _ = torch.cuda.mem_get_info()
     assert free1 == free0
     dx3 = 0.5 ** 3
-    assert float(psi.abs().pow(2).sum()) * dx3 == pytest.approx(1.0, rel=1e-5)
+    assert float(psi64.abs().pow(2).sum()) * dx3 == pytest.approx(1.0, rel=1e-5)
+    assert float(psi128.abs().pow(2).sum()) * dx3 == pytest.approx(1.0, rel=1e-13)
+
+
+@pytest.mark.parametrize("dtype,code", [(torch.complex64, 0), (torch.complex128, 1)])
+def test_zero_or_nonfinite_norm_is_reported_and_psi_left_unchanged(cuda, dtype, code):
+    """The plan path flags a zero norm through its status word; this entry point
+    returns GPE_ERR_NONFINITE and leaves psi as it was (no division by zero)."""
+    so, _lib = lib()
+    n = 16
+    for fill in (0.0, float("nan")):
+        psi = torch.full((n, n, n), fill, dtype=dtype, device="cuda")
+        before = psi.clone()
+        N = ctypes.c_double(-1.0)
+        rc = so.gpe_normalise_noalloc(ctypes.c_void_p(psi.data_ptr()), n, code, 0.25, ctypes.byref(N), stream())
+        assert rc == _lib.GPE_ERR_NONFINITE, rc
+        assert "norm" in _lib.last_error()
+        assert torch.equal(psi.isnan(), before.isnan())
+        assert torch.equal(torch.nan_to_num(psi), torch.nan_to_num(before))
+        # the same status without a norm pointer
+        rc = so.gpe_normalise_noalloc(ctypes.c_void_p(psi.data_ptr()), n, code, 0.25, None, stream())
+        assert rc == _lib.GPE_ERR_NONFINITE
+    # a finite state afterwards is normalised again (the status word was cleared)
+    psi = torch.ones((n, n, n), dtype=dtype, device="cuda")
+    assert so.gpe_normalise_noalloc(ctypes.c_void_p(psi.data_ptr()), n, code, 0.25, None, stream()) == 0
+    assert float(psi.abs().pow(2).sum()) * 0.25 ** 3 == pytest.approx(1.0, rel=1e-5)
 
 
 def test_rejects_sizes_beyond_the_maximum(cuda):
