@@ -80,6 +80,8 @@ struct FastOps {
   int scale;        // FM_Z1: apply the pending renormalisation
   int norm;         // FM_Z2: norm partials and renormalisation scale
   int pdl;          // host: launch as a programmatic dependent of the previous sweep
+  int pf;           // tiles ahead whose lines a block prefetches into L2 (0 = none): the
+                    // tile the block that follows it on the SM will process
 };
 
 // Programmatic dependent launch: a sweep lets the next one start (its blocks
@@ -315,7 +317,10 @@ __device__ __forceinline__ void x_tables(const Phys& ph, int j, int k0, FastTabl
   if (threadIdx.x < L) {
     const int k = k0 + threadIdx.x;
     const double2 a = ph.kin[j], b = ph.kin[k];
-    tb.kyz[threadIdx.x] = ph.kind == 0 ? make_double2(a.x * b.x, 0.0) : cmul(a, b);
+    // the inverse transforms' 1/M rides on the kinetic factor (one multiply per
+    // line instead of one per element in the z sweep that follows)
+    const double2 f = ph.kind == 0 ? make_double2(a.x * b.x, 0.0) : cmul(a, b);
+    tb.kyz[threadIdx.x] = make_double2(f.x * ph.inv_m, f.y * ph.inv_m);
     tb.kyz2[threadIdx.x] = ph.k[j] * ph.k[j] + ph.k[k] * ph.k[k];
   }
 }
@@ -363,11 +368,13 @@ __device__ __forceinline__ void kin_all(typename Cx<R>::T (&v)[EPT], const Phys&
 }
 
 // One local half-step over all registers (layout LANES x VALS, element m = lane +
-// LANES*a, Z tiles: m = z index), potential vz[m] + ctab[l] (+ arrays).  The
-// phases are computed first; which series covers all phases of the warp
-// (|phase| <= 1/8: short series; <= pi/4 (1/2 in imaginary time): full
-// series; else library sincosf/expm1f) is decided once per warp, so each
-// element loop is straight-line code without divergence.
+// LANES*a, Z tiles: m = z index), potential vz[m] + ctab[l] (+ arrays).  complex64:
+// each element whose phase is within the short series' range (|phase| <= 1/8,
+// first omitted terms below 8e-10 of the result) is rotated at once; the others
+// are marked and, only when some lane of the warp has one, rotated in a second
+// pass (full series up to pi/4, 1/2 in imaginary time; library sincosf/expm1f
+// beyond).  No per-element phase array is kept across the two passes, which
+// keeps the fused sweeps within their register budget.
 // TWO: two consecutive real-time half-steps at one point as one rotation by
 // (2 vz[m] + ctab[l] + 2 beta |psi|^2) dt/2 with ctab = c1 + c2; exact because
 // the first rotation leaves |psi| unchanged (callers pass beta already doubled).
@@ -377,10 +384,8 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
                                          const Phys& ph, const FastTables<R>& tb, const R* ctab,
                                          R beta, R h) {
   constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
-  constexpr int E = SLOTS * VALS;
-  R phs[E];
-  R gam[ARR ? E : 1];
-  bool small = true, tiny = true;
+  static_assert(SLOTS * VALS <= 64, "pending mask");
+  unsigned long long pend = 0ull;   // complex64: elements whose phase exceeds the short series' range
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) {
     if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
@@ -392,67 +397,74 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
     for (int a = 0; a < VALS; ++a) {
       const int e = s * VALS + a, m = lane + LANES * a;
       R V = TWO ? (R)2 * tb.vz[m] + c : tb.vz[m] + c;
+      R g = (R)0;
       if (ARR) {
         V += ph.vre ? ((const R*)ph.vre)[row + m] : (R)0;
-        gam[e] = ph.vim ? ((const R*)ph.vim)[row + m] * h : (R)0;
+        g = ph.vim ? ((const R*)ph.vim)[row + m] * h : (R)0;
       }
       const typename Cx<R>::T x = v[e];
-      phs[e] = (V + beta * (x.x * x.x + x.y * x.y)) * h;
-      small = small && fabs(phs[e]) <= (REAL ? (R)0.78539816 : (R)0.5);
-      tiny = tiny && fabs(phs[e]) <= (R)0.125;
-    }
-  }
-  small = __all_sync(0xffffffffu, small);
-  tiny = __all_sync(0xffffffffu, tiny);
-#pragma unroll
-  for (int s = 0; s < SLOTS; ++s) {
-    if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
-#pragma unroll
-    for (int a = 0; a < VALS; ++a) {
-      const int e = s * VALS + a;
-      const typename Cx<R>::T x = v[e];
+      const R phs = (V + beta * (x.x * x.x + x.y * x.y)) * h;
       if (sizeof(R) == 8) {
-        // complex128: library exp / sincos in FP64 (the reference's arithmetic)
         if (!REAL) {
-          const double f = exp(-(double)phs[e]);
+          const double f = exp(-(double)phs);
           v[e] = mk((R)(x.x * f), (R)(x.y * f));
         } else {
           double sd, cd;
-          sincos((double)phs[e], &sd, &cd);
-          if (ARR) { const double am = exp((double)gam[e]); sd *= am; cd *= am; }
+          sincos((double)phs, &sd, &cd);
+          if (ARR) { const double am = exp((double)g); sd *= am; cd *= am; }
           v[e] = mk((R)(x.x * cd + x.y * sd), (R)(x.y * cd - x.x * sd));
         }
-      } else if (tiny) {
+      } else if (fabs(phs) <= (R)0.125) {
         if (!REAL) {
-          const float em = expm1_tiny((float)-phs[e]);
+          const float em = expm1_tiny((float)-phs);
           v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
         } else {
           float sn, cm1;
-          sin_cosm1_tiny((float)phs[e], sn, cm1);
-          if (ARR) { const float am = expm1f((float)gam[e]); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
-          v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
-        }
-      } else if (small) {
-        if (!REAL) {
-          const float em = expm1_series((float)-phs[e]);
-          v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
-        } else {
-          float sn, cm1;
-          sin_cosm1_series((float)phs[e], sn, cm1);
-          if (ARR) { const float am = expm1f((float)gam[e]); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
+          sin_cosm1_tiny((float)phs, sn, cm1);
+          if (ARR) { const float am = expm1f((float)g); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
           v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
         }
       } else {
-        if (!REAL) {
-          const float em = expm1f((float)-phs[e]);
-          v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
+        pend |= 1ull << e;
+      }
+    }
+  }
+  if (sizeof(R) == 8 || !__any_sync(0xffffffffu, pend != 0ull)) return;
+  // second pass over the elements left unrotated: full series up to pi/4 (1/2 in
+  // imaginary time), library functions beyond
+#pragma unroll
+  for (int s = 0; s < SLOTS; ++s) {
+    if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
+    int l, lane;
+    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+    const long long row = tl.base + (long long)l * tl.lstride;
+    const R c = ctab[l];
+#pragma unroll
+    for (int a = 0; a < VALS; ++a) {
+      const int e = s * VALS + a, m = lane + LANES * a;
+      if (!((pend >> e) & 1ull)) continue;
+      R V = TWO ? (R)2 * tb.vz[m] + c : tb.vz[m] + c;
+      R g = (R)0;
+      if (ARR) {
+        V += ph.vre ? ((const R*)ph.vre)[row + m] : (R)0;
+        g = ph.vim ? ((const R*)ph.vim)[row + m] * h : (R)0;
+      }
+      const typename Cx<R>::T x = v[e];
+      const float p = (float)((V + beta * (x.x * x.x + x.y * x.y)) * h);
+      if (!REAL) {
+        const float em = fabsf(p) <= 0.5f ? expm1_series(-p) : expm1f(-p);
+        v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
+      } else {
+        float sn, cm1;
+        if (fabsf(p) <= 0.78539816f) {
+          sin_cosm1_series(p, sn, cm1);
         } else {
           float sh, ch;
-          sincosf(0.5f * (float)phs[e], &sh, &ch);
-          float cm1 = -2.0f * sh * sh, sn = 2.0f * sh * ch;
-          if (ARR) { const float am = expm1f((float)gam[e]); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
-          v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
+          sincosf(0.5f * p, &sh, &ch);
+          cm1 = -2.0f * sh * sh; sn = 2.0f * sh * ch;
         }
+        if (ARR) { const float am = expm1f((float)g); cm1 = am + cm1 + am * cm1; sn = sn + sn * am; }
+        v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
       }
     }
   }
@@ -564,7 +576,7 @@ __device__ __forceinline__ void fast_pointwise(typename Cx<R>::T (&v)[EPT], cons
     half_dispatch<N, AX, R, LANES, VALS, SLOTS, EPT>(v, tl, ph, tb, tb.c1);
     return;
   }
-  scale_all(v, (R)ph.inv_m);
+  // (1/M was applied with the kinetic factor in the x sweep)
   if (MODE == FM_Z21 && ph.kind == 1 && ph.vre == nullptr && ph.vim == nullptr) {
     // real time, potential from tables: the two half-steps as one rotation
     half_all<N, AX, R, LANES, VALS, SLOTS, EPT, true, false, true>(v, tl, ph, tb, tb.c12, (R)(2.0 * ph.beta),
@@ -624,15 +636,32 @@ __device__ __forceinline__ void fast_store(const typename Cx<R>::T (&v)[EPT], co
   }
 }
 
+// Prefetch the lines of tile `tn` into L2 (128-byte lines; z tiles are one
+// contiguous block, y/x tiles N rows of L elements).
+template <int N, int AX, typename R>
+__device__ __forceinline__ void fast_prefetch_l2(const FastTile<N, AX, R>& tn, const void* src) {
+  using C = typename Cx<R>::T;
+  constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
+  const C* base = (const C*)src + tn.base;
+  if (AX == FZ) {
+    constexpr int LINES = L * N * (int)sizeof(C) / 128;
+    for (int q = threadIdx.x; q < LINES; q += T)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(base + q * (128 / (int)sizeof(C))));
+  } else {
+    for (int m = threadIdx.x; m < N; m += T)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(base + (long long)m * tn.nstride));
+  }
+}
+
 // The sweep kernel of one mode.  Register layout before FFT #1: S1 slots of
 // (N1 lanes, N2 values); after FFT #1: S2 slots of (N2 lanes, N1 values) =
 // input layout of FFT #2 with (A, B) = (N2, N1); after FFT #2 the layout is
 // back to (N1 lanes, N2 values).
 //   FM_PLAIN  FFT (inverse if op.inv1; times 1/M if op.invm)       y sweeps, fftn/ifftn
 //   FM_Z1     [scale] half(t1), forward                             first z sweep of a step
-//   FM_Z2     inverse, 1/M, half(t1) [norm partials]                last z sweep of a step
-//   FM_Z21    inverse, 1/M, half(t1), half(t2), forward             last z of a step + first z of the next
-//   FM_XKIN   forward, kinetic, inverse                             x sweep
+//   FM_Z2     inverse, half(t1) [norm partials]                     last z sweep of a step
+//   FM_Z21    inverse, half(t1), half(t2), forward                  last z of a step + first z of the next
+//   FM_XKIN   forward, kinetic x 1/M, inverse                       x sweep (carries the step's 1/M)
 //   FM_DIAGR  real-space sums (N, E_pot, E_int), forward            diagnostic z sweep (to the work buffer)
 //   FM_DIAGK  forward, k-space sums (E_kin [, shells]), no store     diagnostic x sweep
 template <int N, int AX, typename R, int MODE, bool CG = false>
@@ -713,6 +742,10 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
 
   C v[EPT];
   fast_load<N, AX, R, S1, CG>(v, tl, (const C*)sw.src, MODE == FM_Z2 || MODE == FM_Z21 || (MODE == FM_PLAIN && op.inv1));
+  // Bring the tile of the next wave's block on this SM into L2 while this one
+  // computes: one wave ahead (tile + resident blocks), measured 51.2 -> 46.4 us
+  // for the y sweep at 256^3 (two waves ahead was slower).
+  if (!CG && op.pf > 0 && tile + op.pf < ntiles) fast_prefetch_l2<N, AX, R>(FastTile<N, AX, R>(tile + op.pf), sw.src);
   prologue();
   __syncthreads();  // twiddles and tables visible
   if (MODE == FM_Z1) fast_pointwise<N, AX, R, MODE, 0, N1, N2, S1>(v, tl, ph, tb, op, cx);
@@ -753,7 +786,10 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
 // Resident blocks per SM that the register allocation must allow, 0 = the
 // compiler's choice.  Measured for complex64 at n = 128, 256: the plain FFT
 // sweeps are memory-bound and want 1024 threads per SM (64 registers at
-// T = 256); the fused modes keep 768 (85 registers) for their extra live state.
+// T = 256); the fused modes keep 768 (80 registers) for their extra live state,
+// except Z21 and XKIN at n = 256, which run 4 blocks of 64 registers (a few
+// hundred bytes of spills in Z21): 4486 -> 4541 steps/s at 256^3, the gain
+// being in the overlap of the programmatically launched sweeps.
 // At n = 512 (32-point phase, up to 214 registers unbounded; 512-thread
 // blocks) one block per SM: plain sweeps 95 registers, fused ones 128 with a
 // few hundred bytes of spills in Z21/Z2 (bounds measured 240 -> 291 steps/s at
@@ -761,7 +797,9 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
 // The diagnostic z sweep (FP64 potential per point) keeps 512 threads per SM.
 template <int N, typename R, int MODE> struct FastBounds {
   static constexpr int value = (sizeof(R) == 4 && (N == 128 || N == 256))
-                                   ? (MODE == FM_PLAIN ? 1024 : MODE == FM_DIAGR ? 512 : 768) / FastCfg<N, R>::T
+                                   ? (MODE == FM_PLAIN ? 1024 : MODE == FM_DIAGR ? 512
+                                      : (N == 256 && (MODE == FM_Z21 || MODE == FM_XKIN)) ? 1024 : 768) /
+                                         FastCfg<N, R>::T
                                : (sizeof(R) == 4 && N == 512)
                                    ? (MODE == FM_PLAIN ? 768 : 512) / FastCfg<N, R>::T : 0;
 };

@@ -18,21 +18,36 @@ template <int N, int AX, typename R, int MODE> constexpr auto fast_batch_kernel(
   else return &k_fast_batch<N, AX, R, MODE>;
 }
 
+// Blocks of `kern` resident on the whole device at once (the L2 prefetch
+// distance of a sweep: the tile the next block on an SM will take).
+template <typename K>
+static cudaError_t resident_blocks(K kern, int threads, size_t smem, int& out) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  out = e == cudaSuccess ? sms * per_sm : 0;
+  return e;
+}
+
 template <int N, int AX, typename R, int MODE>
-static cudaError_t launch_fast_one(const Phys& ph, const Sweep& sw, const FastOps& op, cudaStream_t st) {
+static cudaError_t launch_fast_one(const Phys& ph, const Sweep& sw, const FastOps& op_in, cudaStream_t st) {
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
   const int tiles = AX == FZ ? N * N / L : N * (N / L);
   constexpr size_t smem = fast_smem_bytes<N, R>();
   constexpr auto kern = fast_kernel<N, AX, R, MODE>();
-  static int attr_dev = -1;
+  static int attr_dev = -1, resident = 0;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = resident_blocks(kern, T, smem, resident);
     if (e != cudaSuccess) return e;
     attr_dev = dev;
   }
+  FastOps op = op_in;
+  op.pf = resident < tiles ? resident : 0;
   if (!op.pdl) {
     kern<<<tiles, T, smem, st>>>(ph, sw, op);
     return cudaGetLastError();
@@ -67,21 +82,26 @@ cudaError_t launch_fast_n(int ax, const Phys& ph, const Sweep& sw, const FastOps
 }
 
 template <int N, int AX, typename R, int MODE>
-static cudaError_t launch_fastb_one(const Phys* phs, const Sweep* sws, int count, const FastOps& op,
+static cudaError_t launch_fastb_one(const Phys* phs, const Sweep* sws, int count, const FastOps& op_in,
                                     cudaStream_t st) {
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
   const int tiles = AX == FZ ? N * N / L : N * (N / L);
   constexpr size_t smem = fast_smem_bytes<N, R>();
   constexpr auto kern = fast_batch_kernel<N, AX, R, MODE>();
-  static int attr_dev = -1;
+  static int attr_dev = -1, resident = 0;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = resident_blocks(kern, T, smem, resident);
     if (e != cudaSuccess) return e;
     attr_dev = dev;
   }
+  // blocks run x (tile) fastest, so the next block on an SM takes tile + resident
+  // of the same instance while the instance has that many tiles left
+  FastOps op = op_in;
+  op.pf = resident < tiles ? resident : 0;
   kern<<<dim3(tiles, count), T, smem, st>>>(phs, sws, op);
   return cudaGetLastError();
 }

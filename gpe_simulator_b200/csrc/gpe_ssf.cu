@@ -641,7 +641,7 @@ int psweep(gpe_plan* p, void* psi, int mz, const FastOps* ops, int nstage, int z
 
 FastOps mk_ops(int mode, int inv1 = 0, int invm = 0, int scale = 0, int norm = 0) {
   FastOps o;
-  o.mode = mode; o.inv1 = inv1; o.invm = invm; o.scale = scale; o.norm = norm; o.pdl = 0;
+  o.mode = mode; o.inv1 = inv1; o.invm = invm; o.scale = scale; o.norm = norm; o.pdl = 0; o.pf = 0;
   return o;
 }
 
