@@ -333,11 +333,81 @@ def ours(args, world, rank, local):
         result["plain_floor"] = plain_floor_leg()
     if world == 1 and not args.no_large:
         result["stir512"] = large_leg()
+    if world == 1 and not args.no_expr:
+        result["expression_beam"] = expression_leg()
     if world == 1 and not args.no_batch:
         result["batched"] = batched_leg()
     if world == 1 and not args.no_serve:
         result["serving"] = serving_leg(args.serve_requests, args.serve_rate)
     return result, plan
+
+
+def expression_leg(steps=200, warmup=5):
+    """The stirring beam written in the reference's expression grammar (the form a
+    YAML stage carries, ``gpe/make_kernel.py:14-45``) against the built-in beam,
+    256^3 complex64, same state: steps/s of one multi-step call and of per-step
+    ``make_real_propagator`` closure calls, state resident, and the relative
+    difference of the two final states."""
+    import torch
+    from types import SimpleNamespace
+    from gpe_simulator_b200 import Plan, beam_in_reference_units
+    from gpe_simulator_b200.expressions import cuda_expression
+    from gpe_simulator_b200.make_propagator import make_real_propagator
+    from gpe_simulator_b200.plan import launch_count
+    x, k = grids()
+    beam = beam_in_reference_units(BEAM["amp"], BEAM["width"], BEAM["radius"], BEAM["omega"],
+                                   BEAM["ramp_steps"] * DT)
+    expr = beam.expression()
+    g = torch.from_numpy(np.exp(-x ** 2 / 2)).cuda()
+    base = (g[:, None, None] * g[None, :, None] * g[None, None, :]).to(torch.complex64).contiguous()
+    out = {"expression": expr}
+    finals = {}
+    for name, kw in (("builtin", dict(beam=beam)), ("expression", dict(dynamic_expr=expr))):
+        plan = Plan(N_GRID, x, k, dtype=torch.complex64, kind="real", beta=2 * G, dt=DT / 2,
+                    static_expr=TRAP_REF, **kw)
+        psi = base.clone()
+        plan.normalise(psi)
+        plan.step(psi, warmup, 0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        n0 = launch_count(plan)
+        e0.record()
+        plan.step(psi, steps, warmup)
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"{name}_steps_per_s"] = steps * 1e3 / e0.elapsed_time(e1)
+        out[f"{name}_launches_per_step"] = (launch_count(plan) - n0) / steps
+        finals[name] = psi
+        plan.close()
+        # the drop-in closure, one call per step (as gpe/launch.py:8-13 calls it)
+        pp = dict(static=dict(activate=True, expression=cuda_expression(TRAP_REF)),
+                  dynamic=dict(activate=name == "expression",
+                               expression=cuda_expression(expr, True) if name == "expression" else "0"))
+        st = SimpleNamespace(type="real", N_grids=N_GRID, beta=2 * G, dt=DT / 2, kinetic_coeff=1.0,
+                             beam=beam if name == "builtin" else None,
+                             x_array=torch.from_numpy(x).cuda(), k_array=torch.from_numpy(k).cuda(),
+                             staticV=torch.zeros((N_GRID,) * 3, dtype=torch.complex128, device="cuda"),
+                             potential_params=pp, k_cut_params=dict(activate=False, k_cut=0.0),
+                             psi=base.clone())
+        prop = make_real_propagator(st)
+        for i in range(warmup):
+            prop(st, i * st.dt)
+        torch.cuda.synchronize()
+        e0.record()
+        for i in range(steps):
+            prop(st, (warmup + i) * st.dt)
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"{name}_closure_steps_per_s"] = steps * 1e3 / e0.elapsed_time(e1)
+        del st, prop
+    d = finals["expression"].to(torch.complex128) - finals["builtin"].to(torch.complex128)
+    out["rel_diff_final_psi"] = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(
+        finals["builtin"].to(torch.complex128)))
+    out["ratio_multistep"] = out["expression_steps_per_s"] / out["builtin_steps_per_s"]
+    out["ratio_closure"] = out["expression_closure_steps_per_s"] / out["builtin_closure_steps_per_s"]
+    out["steps"] = steps
+    torch.cuda.empty_cache()
+    return out
 
 
 def large_leg(steps=100, warmup=5):
@@ -545,6 +615,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 512^3 leg")
+    ap.add_argument("--no-expr", action="store_true",
+                    help="skip the leg with the beam as a reference-grammar expression")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the floor of the reference's step sequence (cuFFT via torch.fft)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")

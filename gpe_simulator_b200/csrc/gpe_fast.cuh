@@ -301,6 +301,12 @@ __device__ __forceinline__ void z_tables(const Phys& ph, const Sweep& sw, int a0
         b2 = (R)ph.beam_amp * rexp(-ex * ex * iw) * rexp(-ey * ey * iw);
       }
     }
+    if (ph.ltab) {
+      // dynamic potential without z terms: this line's values at t1, t2
+      const R* lt = (const R*)ph.ltab;
+      b1 += lt[g];
+      if (two) b2 += lt[(long long)N * N + g];
+    }
     tb.c1[threadIdx.x] = base + b1;
     tb.c2[threadIdx.x] = base + b2;
     tb.c12[threadIdx.x] = (base + b1) + (base + b2);
@@ -491,7 +497,7 @@ __device__ __forceinline__ void half_dispatch(typename Cx<R>::T (&v)[EPT], const
 // plain FP64, the thread sums added with compensation.
 template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT>
 __device__ __forceinline__ void diag_real_all(const typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
-                                              const Phys& ph, PwCtx<R>& cx) {
+                                              const Phys& ph, const FastTables<R>& tb, PwCtx<R>& cx) {
   constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) {
@@ -506,7 +512,10 @@ __device__ __forceinline__ void diag_real_all(const typename Cx<R>::T (&v)[EPT],
       tl.coords(l, m, i, j, k);
       const typename Cx<R>::T x = v[s * VALS + a];
       const double rho = (double)x.x * x.x + (double)x.y * x.y;
-      const double V = (double)potential<R>(ph, N, i, j, k, tl.gidx(l, m), cx.t1, cx.b1x, cx.b1y);
+      // with a line program the potential comes from the z-sweep tables (static
+      // axes and line terms at t1), plus the static array
+      const double V = ph.ltab ? (double)(tb.vz[m] + tb.c1[l] + (ph.vre ? ((const R*)ph.vre)[tl.gidx(l, m)] : (R)0))
+                                : (double)potential<R>(ph, N, i, j, k, tl.gidx(l, m), cx.t1, cx.b1x, cx.b1y);
       n0 += rho;
       n1 = fma(V, rho, n1);
       n2 = fma(rho, rho, n2);
@@ -711,7 +720,7 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
         t2[q] = entry(n2 * k2b);
       }
     }
-    if (ZM) z_tables<N, R>(ph, sw, tl.a0, tb, MODE == FM_Z21);
+    if (ZM || (MODE == FM_DIAGR && ph.ltab)) z_tables<N, R>(ph, sw, tl.a0, tb, MODE == FM_Z21);
     if (MODE == FM_XKIN) x_tables<N, R>(ph, tl.a0, tl.b0, tb);
     // diagnostic x sweep: the shell histogram takes the tables region
     if (MODE == FM_DIAGK && sw.hist)
@@ -749,7 +758,7 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   prologue();
   __syncthreads();  // twiddles and tables visible
   if (MODE == FM_Z1) fast_pointwise<N, AX, R, MODE, 0, N1, N2, S1>(v, tl, ph, tb, op, cx);
-  if (MODE == FM_DIAGR) diag_real_all<N, AX, R, N1, N2, S1>(v, tl, ph, cx);
+  if (MODE == FM_DIAGR) diag_real_all<N, AX, R, N1, N2, S1>(v, tl, ph, tb, cx);
   fft_2phase<N, N1, N2, AX, R, S1, S2, EPT>(v, ex, t1);
   if (MODE == FM_Z21 || MODE == FM_XKIN) {
     if (MODE == FM_Z21) conj_all(v);  // finish the inverse before the physics

@@ -23,6 +23,13 @@ enum : unsigned {
 
 enum Axis : int { AX_Z = 0, AX_Y = 1, AX_X = 2 };
 
+// Internal opcodes of the line programs the host derives from a dynamic
+// potential (beyond the public ones of gpe_ssf.h): square of the top of the
+// stack, and push of slot k (OP_SLOT0 + k).
+constexpr int OP_SQR = 40;
+constexpr int OP_SLOT0 = 64;
+#define GPE_LINE_SLOTS 8
+
 // status bits
 enum : int { ST_NONFINITE = 1, ST_TIMEOUT = 2, ST_LAYOUT = 4 };  // ST_LAYOUT: a sweep refused its shared-memory layout
 
@@ -39,6 +46,10 @@ struct Phys {
   const void* vim;       // [n^3] static imaginary part (real time), precision R (nullable)
   const double* dyn;     // dynamic bytecode (nullable)
   int dyn_len;
+  // register-resident sweeps: the dynamic potential when none of its terms depends
+  // on z, per z-line (i n + j) at the two half-step times of the next z sweep:
+  // [2][n*n] in precision R, filled by k_line_table right before that sweep
+  const void* ltab;
   int beam;
   double beam_amp, beam_inv_w2, beam_radius, beam_omega, beam_t_ramp;
   int kcut;
@@ -67,6 +78,13 @@ struct Sweep {
   int nbins;             // diag k-space: number of shells
   double shell_w;        // shell width
   double* hist;          // per-block shell histograms [gridDim][nbins]
+};
+
+// Values of a line program's slots (its time-dependent subexpressions, FP64,
+// evaluated on the host) at the two half-step times of one z sweep.
+struct LineSlots {
+  double s1[GPE_LINE_SLOTS];
+  double s2[GPE_LINE_SLOTS];
 };
 
 // ---------------------------------------------------------------- helpers
@@ -125,8 +143,10 @@ __device__ void block_merge(Acc (&a)[NV], Acc* sh /* [32*NV] */) {
   __syncthreads();
 }
 
-// Potential-expression stack machine (FP64).
-static __device__ double eval_program(const double* prog, int len, double x, double y, double z, double t) {
+// Potential-expression stack machine (FP64); `slots` serves the internal
+// OP_SLOT0 + k pushes of line programs (null for the public bytecode).
+static __device__ double eval_program(const double* prog, int len, double x, double y, double z, double t,
+                                      const double* slots = nullptr) {
   double st[32];
   int sp = 0;
   for (int pc = 0; pc < len;) {
@@ -151,12 +171,34 @@ static __device__ double eval_program(const double* prog, int len, double x, dou
       case 18: st[sp - 1] = tanh(st[sp - 1]); break;
       case 19: st[sp - 1] = fabs(st[sp - 1]); break;
       case 20: st[sp - 1] = log(st[sp - 1]); break;
-      default: break;
+      case OP_SQR: st[sp - 1] = st[sp - 1] * st[sp - 1]; break;
+      default:
+        if (slots && op >= OP_SLOT0 && op < OP_SLOT0 + GPE_LINE_SLOTS) st[sp++] = slots[op - OP_SLOT0];
+        break;
     }
     if (sp < 1) sp = 1;
     if (sp > 31) sp = 31;
   }
   return st[0];
+}
+
+// The dynamic potential of every z-line (i n + j) at t1 (and t2 when `two`),
+// FP64 evaluation of the line program stored in precision R: one thread per
+// line and time.  Launched as a programmatic dependent of the sweep before it,
+// it waits for that sweep (the z sweep that last read the table has finished by
+// then) and lets the z sweep after it launch early.
+template <typename R>
+__global__ void __launch_bounds__(256) k_line_table(const double* __restrict__ prog, int len,
+                                                    const double* __restrict__ x, int n, LineSlots sl,
+                                                    R* __restrict__ tab, int two) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const long long nn = (long long)n * n;
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (two ? 2 : 1) * nn) return;
+  const int which = (int)(q / nn);
+  const long long l = q - which * nn;
+  tab[q] = (R)eval_program(prog, len, x[l / n], x[l % n], 0.0, 0.0, which ? sl.s2 : sl.s1);
 }
 
 // Beam centre for a time; angle accumulated in FP64.

@@ -85,6 +85,129 @@ double host_eval(const std::vector<double>& prog, double x, double y, double z, 
   return sp ? st[0] : 0.0;
 }
 
+// ---- dynamic potentials on the register-resident sweeps
+// A dynamic potential V(x, y, z, t) whose additive terms do not depend on z is
+// constant along every z-line at a given time, so the z sweeps can take it per
+// line instead of per point (a stirring beam rotating in the x-y plane is of
+// this form).  The bytecode is read back into a tree; every subexpression that
+// depends on t alone becomes a slot (evaluated on the host in FP64 once per
+// launch, at each half-step time), constant subexpressions are folded, and
+// powers 2 become squares.  What remains is a short program in (x, y) that the
+// z sweeps evaluate once per line in FP64.
+struct ExprNode {
+  int op = 0;
+  double val = 0.0;
+  int a = -1, b = -1;
+  unsigned vars = 0;   // 1 x, 2 y, 4 z, 8 t
+};
+
+bool expr_tree(const std::vector<double>& prog, std::vector<ExprNode>& nodes, int& root) {
+  std::vector<int> st;
+  for (size_t pc = 0; pc < prog.size();) {
+    ExprNode nd;
+    nd.op = (int)prog[pc++];
+    switch (nd.op) {
+      case GPE_OP_CONST: nd.val = prog[pc++]; break;
+      case GPE_OP_X: nd.vars = 1; break;
+      case GPE_OP_Y: nd.vars = 2; break;
+      case GPE_OP_Z: nd.vars = 4; break;
+      case GPE_OP_T: nd.vars = 8; break;
+      case GPE_OP_ADD: case GPE_OP_SUB: case GPE_OP_MUL: case GPE_OP_DIV: case GPE_OP_POW:
+        if (st.size() < 2) return false;
+        nd.b = st.back(); st.pop_back();
+        nd.a = st.back(); st.pop_back();
+        nd.vars = nodes[nd.a].vars | nodes[nd.b].vars;
+        break;
+      default:   // unary
+        if (st.empty()) return false;
+        nd.a = st.back(); st.pop_back();
+        nd.vars = nodes[nd.a].vars;
+        break;
+    }
+    nodes.push_back(nd);
+    st.push_back((int)nodes.size() - 1);
+  }
+  if (st.size() != 1) return false;
+  root = st[0];
+  return true;
+}
+
+void expr_emit_plain(const std::vector<ExprNode>& nodes, int i, std::vector<double>& out) {
+  const ExprNode& nd = nodes[i];
+  if (nd.a >= 0) expr_emit_plain(nodes, nd.a, out);
+  if (nd.b >= 0) expr_emit_plain(nodes, nd.b, out);
+  out.push_back((double)nd.op);
+  if (nd.op == GPE_OP_CONST) out.push_back(nd.val);
+}
+
+// Residual line program of node i: t-only subtrees become slots, constant
+// subtrees constants, x^2 a square.  False when the slot budget runs out.
+bool expr_emit_line(const std::vector<ExprNode>& nodes, int i, std::vector<double>& out,
+                    std::vector<std::vector<double>>& slots) {
+  const ExprNode& nd = nodes[i];
+  if (nd.vars == 0 && nd.op != GPE_OP_CONST) {
+    std::vector<double> sub;
+    expr_emit_plain(nodes, i, sub);
+    out.push_back(GPE_OP_CONST);
+    out.push_back(host_eval(sub, 0.0, 0.0, 0.0, 0.0));
+    return true;
+  }
+  if (nd.vars == 8) {
+    if ((int)slots.size() == GPE_LINE_SLOTS) return false;
+    std::vector<double> sub;
+    expr_emit_plain(nodes, i, sub);
+    slots.push_back(sub);
+    out.push_back((double)(OP_SLOT0 + (int)slots.size() - 1));
+    return true;
+  }
+  if (nd.op == GPE_OP_POW && nodes[nd.b].vars == 0) {
+    std::vector<double> sub;
+    expr_emit_plain(nodes, nd.b, sub);
+    if (host_eval(sub, 0.0, 0.0, 0.0, 0.0) == 2.0) {
+      if (!expr_emit_line(nodes, nd.a, out, slots)) return false;
+      out.push_back((double)OP_SQR);
+      return true;
+    }
+  }
+  if (nd.a >= 0 && !expr_emit_line(nodes, nd.a, out, slots)) return false;
+  if (nd.b >= 0 && !expr_emit_line(nodes, nd.b, out, slots)) return false;
+  out.push_back((double)nd.op);
+  if (nd.op == GPE_OP_CONST) out.push_back(nd.val);
+  return true;
+}
+
+// Line form of a dynamic program: true (with `line` and `slots` filled) when no
+// additive term depends on z.
+bool dynamic_line_form(const std::vector<double>& prog, std::vector<double>& line,
+                       std::vector<std::vector<double>>& slots) {
+  std::vector<ExprNode> nodes;
+  int root = -1;
+  if (!expr_tree(prog, nodes, root)) return false;
+  // signed top-level terms of the sum
+  std::vector<std::pair<int, int>> terms;
+  std::vector<std::pair<int, int>> todo{{root, 1}};
+  while (!todo.empty()) {
+    const auto [i, sign] = todo.back();
+    todo.pop_back();
+    const ExprNode& nd = nodes[i];
+    if (nd.op == GPE_OP_ADD) { todo.push_back({nd.b, sign}); todo.push_back({nd.a, sign}); }
+    else if (nd.op == GPE_OP_SUB) { todo.push_back({nd.b, -sign}); todo.push_back({nd.a, sign}); }
+    else if (nd.op == GPE_OP_NEG) todo.push_back({nd.a, -sign});
+    else terms.push_back({i, sign});
+  }
+  line.clear();
+  slots.clear();
+  bool first = true;
+  for (const auto& [i, sign] : terms) {
+    if (nodes[i].vars & 4) return false;
+    if (!expr_emit_line(nodes, i, line, slots)) return false;
+    if (sign < 0) line.push_back(GPE_OP_NEG);
+    if (!first) line.push_back(GPE_OP_ADD);
+    first = false;
+  }
+  return (int)line.size() <= GPE_PROGRAM_MAX;
+}
+
 // Validate a program: known opcodes, operands present, stack within bounds, one result.
 bool check_program(const double* p, int len, std::string& why) {
   if (len == 0) return true;
@@ -371,6 +494,8 @@ struct gpe_plan {
   size_t csize = 8;                // bytes per complex element
   std::vector<double> x, k;
   std::vector<double> prog_static_g, prog_dyn;
+  std::vector<double> prog_line;                   // dynamic potential per z-line (register-resident sweeps)
+  std::vector<std::vector<double>> slot_progs;     // its time-dependent subexpressions (host, per launch)
   PassPlan pp{};
   Phys ph{};
   int lt_z = 1, lt_yx = 16;
@@ -398,6 +523,8 @@ struct gpe_plan {
   void* d_vim = nullptr;
   double* d_prog_g = nullptr;
   double* d_dyn = nullptr;
+  double* d_line = nullptr;
+  void* d_ltab = nullptr;          // [2][n*n] per-line dynamic potential (line form), precision of psi
   void* d_tw = nullptr;
   double* d_partial = nullptr;   // 2 areas of 4*max_tiles doubles
   unsigned* d_ticket = nullptr;
@@ -496,6 +623,43 @@ void beam_centres(const gpe_plan* p, Sweep& sw) {
   centre(sw.t2, sw.bc2x, sw.bc2y);
 }
 
+// The line table of the next z sweep: the line program's slot values at t1
+// (and t2) in FP64 on the host, then one thread per z-line and time on the
+// device.  Inside a step sequence it is a programmatic dependent of the sweep
+// before it, and the z sweep after it is one of it.
+int line_table(gpe_plan* p, double t1, double t2, bool two, cudaStream_t st) {
+  LineSlots sl;
+  memset(&sl, 0, sizeof(sl));
+  for (size_t k = 0; k < p->slot_progs.size(); ++k) {
+    sl.s1[k] = host_eval(p->slot_progs[k], 0.0, 0.0, 0.0, t1);
+    sl.s2[k] = host_eval(p->slot_progs[k], 0.0, 0.0, 0.0, t2);
+  }
+  const long long count = (two ? 2LL : 1LL) * p->n * p->n;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)((count + 255) / 256));
+  cfg.blockDim = dim3(256);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = p->pdl_chain && p->pdl_prev && !p->prof ? 1 : 0;
+  const double* prog = p->d_line;
+  const int len = (int)p->prog_line.size();
+  const cudaError_t e =
+      p->dtype == GPE_C64
+          ? cudaLaunchKernelEx(&cfg, k_line_table<float>, prog, len, (const double*)p->d_x, p->n, sl,
+                               (float*)p->d_ltab, two ? 1 : 0)
+          : cudaLaunchKernelEx(&cfg, k_line_table<double>, prog, len, (const double*)p->d_x, p->n, sl,
+                               (double*)p->d_ltab, two ? 1 : 0);
+  if (e != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("line table: ") + cudaGetErrorString(e));
+  ++p->launches;
+  p->pdl_prev = p->pdl_chain;
+  return GPE_OK;
+}
+
+bool needs_lines(int mode) { return mode == FM_Z1 || mode == FM_Z2 || mode == FM_Z21 || mode == FM_DIAGR; }
+
 int sweep(gpe_plan* p, int ax, const Sweep& sw_in, cudaStream_t st) {
   Sweep sw = sw_in;
   beam_centres(p, sw);
@@ -568,6 +732,7 @@ const CUtensorMap* tma_maps(gpe_plan* p, const void* base, int fax) {
 // Register-resident sweep (n with a fast split); same accounting as sweep().
 int fsweep(gpe_plan* p, int ax, Sweep sw, const FastOps& op, cudaStream_t st) {
   beam_centres(p, sw);
+  if (p->d_ltab && needs_lines(op.mode)) TRY(line_table(p, sw.t1, sw.t2, op.mode == FM_Z21, st));
   sw.pp = p->pp;
   sw.tw = p->d_tw;
   sw.tw_lo = (const char*)p->d_tw + (size_t)p->n * p->csize;
@@ -609,6 +774,7 @@ int psweep(gpe_plan* p, void* psi, int mz, const FastOps* ops, int nstage, int z
   sw.t1 = t1;
   sw.t2 = t2;
   beam_centres(p, sw);
+  if (p->d_ltab) TRY(line_table(p, t1, t2, mz == FM_Z21, st));
   sw.partial = p->d_partial;
   sw.pp = p->pp;
   sw.tw = p->d_tw;
@@ -738,10 +904,13 @@ int fill_plan(gpe_plan* p, const gpe_desc* d) {
   // (complex64 plans that evaluate the local factor in FP64 use the generic sweeps,
   // which carry that variant; keeping it out of the register-resident kernels keeps
   // their register budget)
+  // a dynamic potential stays on them when none of its terms depends on z (line form)
+  const bool line_ok = d->dynamic_g_len == 0 || dynamic_line_form(p->prog_dyn, p->prog_line, p->slot_progs);
   p->fast = (n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 160 || n == 256 ||
              (n == 512 && d->dtype == GPE_C64)) &&
-            d->generic_only != 1 && d->dynamic_g_len == 0 && !(d->local_fp64 && d->dtype == GPE_C64) &&
+            d->generic_only != 1 && line_ok && !(d->local_fp64 && d->dtype == GPE_C64) &&
             !d->exact_local;
+  if (!p->fast) { p->prog_line.clear(); p->slot_progs.clear(); }
   p->plane = p->fast && d->dtype == GPE_C64 && (n == 128 || n == 256) && d->generic_only == 3;
   p->tma = p->fast && d->dtype == GPE_C64 && (n == 128 || n == 256) && d->generic_only == 4;
   const int emax = 512 * p->ept;
@@ -829,7 +998,7 @@ int build_static(gpe_plan* p, const void* v, int v_kind, cudaStream_t st) {
 void free_plan(gpe_plan* p) {
   for (auto& r : p->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   for (auto e : p->pool) cudaEventDestroy(e);
-  void* bufs[] = {p->d_x, p->d_k, p->d_kin, p->d_kth, p->d_vax, p->d_vre, p->d_vim, p->d_prog_g, p->d_dyn,
+  void* bufs[] = {p->d_x, p->d_k, p->d_kin, p->d_kth, p->d_vax, p->d_vre, p->d_vim, p->d_prog_g, p->d_dyn, p->d_line, p->d_ltab,
                   p->d_tw, p->d_partial, p->d_ticket, p->d_scale, p->d_status, p->d_hist, p->d_out,
                   p->d_work, p->d_plane, p->d_proj};
   for (void* b : bufs)
@@ -870,6 +1039,11 @@ int create(const gpe_desc* d, gpe_plan** out) {
     CU(cudaMalloc(&p->d_dyn, p->prog_dyn.size() * sizeof(double)));
     CU(cudaMemcpy(p->d_dyn, p->prog_dyn.data(), p->prog_dyn.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
+  if (!p->prog_line.empty()) {
+    CU(cudaMalloc(&p->d_line, p->prog_line.size() * sizeof(double)));
+    CU(cudaMemcpy(p->d_line, p->prog_line.data(), p->prog_line.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMalloc(&p->d_ltab, 2 * (size_t)n * n * (p->dtype == GPE_C64 ? 4 : 8)));
+  }
   CU(cudaMalloc(&p->d_partial, 2 * 4 * (size_t)p->max_tiles * sizeof(double)));
   CU(cudaMalloc(&p->d_ticket, sizeof(unsigned)));
   CU(cudaMemset(p->d_ticket, 0, sizeof(unsigned)));
@@ -897,6 +1071,7 @@ int create(const gpe_desc* d, gpe_plan** out) {
   ph.vax = p->d_vax;
   ph.dyn = p->d_dyn;
   ph.dyn_len = (int)p->prog_dyn.size();
+  ph.ltab = p->d_ltab;
   ph.beam = d->beam_enabled ? 1 : 0;
   ph.beam_amp = d->beam_amp;
   ph.beam_inv_w2 = d->beam_enabled ? 1.0 / (d->beam_width * d->beam_width) : 0.0;

@@ -32,6 +32,20 @@ class Beam:
     omega: float
     t_ramp: float = 0.0
 
+    def expression(self):
+        """The same beam in the reference's potential grammar (``x, y, t``, ``abs``,
+        ``cos``, ``sin``, ``exp``): ``min(t, t_ramp)`` written as
+        ``(t + t_ramp - abs(t - t_ramp))/2``.  A plan given this as its dynamic
+        expression runs the register-resident sweeps as with the built-in beam."""
+        r = repr
+        if self.t_ramp > 0:
+            m = f"((t+{r(self.t_ramp)}-abs(t-{r(self.t_ramp)}))/2)"
+            th = f"({r(self.omega)}*({m}**2/(2*{r(self.t_ramp)})+t-{m}))"
+        else:
+            th = f"({r(self.omega)}*t)"
+        return (f"{r(self.amp)}*exp(-((x-{r(self.radius)}*cos({th}))**2"
+                f"+(y-{r(self.radius)}*sin({th}))**2)/{r(self.width)}**2)")
+
 
 _DTYPES = {torch.complex64: _lib.C64, torch.complex128: _lib.C128}
 
