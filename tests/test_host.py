@@ -29,6 +29,35 @@ def test_cuda_expression_matches_reference_rendering():
         cuda_expression("x; return 0")
 
 
+def test_expression_front_end_matches_the_reference_renderings():
+    """Every formula of the fixture (generated by the reference's own
+    ``cuda_expression``, ``tests/golden/make_expr_cases.py``) renders to the same
+    CUDA text here, and what the reference rejects is rejected here too."""
+    import json
+    from gpe_simulator_b200.expressions import cuda_expression
+    rows = json.loads((ROOT / "tests" / "golden" / "expr_cases.json").read_text())
+    assert len(rows) > 40
+    for row in rows:
+        if row["cuda"] is None:
+            with pytest.raises(ValueError):
+                cuda_expression(row["source"], row["time_dependent"])
+        else:
+            assert cuda_expression(row["source"], row["time_dependent"]) == row["cuda"], row["source"]
+
+
+def test_expression_limits_come_from_the_device_evaluator():
+    from gpe_simulator_b200.expressions import compile_program, STACK_MAX, PROGRAM_MAX
+    deep = "x*" + "(y+" * STACK_MAX + "z" + ")" * STACK_MAX
+    with pytest.raises(ValueError, match="stack"):
+        compile_program(deep)
+    long_sum = "+".join(["x*y"] * (PROGRAM_MAX // 2))
+    with pytest.raises(ValueError, match="at most"):
+        compile_program(long_sum)
+    with pytest.raises(ValueError, match="nested"):
+        compile_program("(" * 150 + "x" + ")" * 150)
+    assert compile_program("0") == [] and compile_program("-(0.0)") == []
+
+
 def run_program(prog, x, y, z, t=0.0):
     """Python model of the device stack machine (same opcodes as include/gpe_ssf.h)."""
     st = []
