@@ -338,7 +338,7 @@ def ours(args, world, rank, local):
     if world == 1 and not args.no_batch:
         result["batched"] = batched_leg()
     if world == 1 and not args.no_serve:
-        result["serving"] = serving_leg(args.serve_requests, args.serve_rate)
+        result["serving"] = serving_leg(args.serve_requests, args.serve_rates, args.serve_plain_sample)
     return result, plan
 
 
@@ -490,6 +490,65 @@ def plain_floor_leg(steps=50, warmup=5):
     return out
 
 
+def plain_form_solve_ms(n, steps, check_every, dtype, real_time=False):
+    """Device milliseconds of one solve in the reference's plain form on this GPU
+    (CuPy is not installed here, so its own code cannot run): per step, looped
+    from Python as ``gpe/launch.py:8-13`` loops, the kernel sequence of
+    ``gpe/make_propagator.py:109-151`` (``57-103`` in real time) -- half-step,
+    ``fftn``, kinetic factor, ``ifftn``, half-step, and in imaginary time the
+    two-pass norm and the division of ``gpe/helper.py:81-93`` -- plus, every
+    ``check_every`` steps, the energy check of the convergence rule (``fftn`` of
+    the state and the E_kin, E_pot, E_int sums).  cuFFT runs through torch.fft;
+    each elementwise RawKernel is one torch kernel moving the same bytes (the
+    half-step reads psi and its potential array and writes psi), so the
+    reference's own solve cannot be faster.  ``steps`` is the step count the
+    solve needs (taken from the batched run, which computes the same physics)."""
+    import torch
+    real = torch.float64 if dtype == torch.complex128 else torch.float32
+    g = torch.Generator(device="cuda").manual_seed(n)
+    psi = torch.randn((n, n, n), dtype=dtype, device="cuda", generator=g)
+    psi /= torch.linalg.vector_norm(psi)
+    # the half-step's potential array (float64 in imaginary time, complex128 U - iGamma in
+    # real time) and a unit-modulus stand-in factor for the arithmetic
+    if real_time:
+        pot = torch.polar(torch.ones((n, n, n), dtype=real, device="cuda"),
+                          torch.randn((n, n, n), dtype=real, device="cuda", generator=g))
+    else:
+        pot = torch.ones((n, n, n), dtype=real, device="cuda")
+    k2 = torch.rand((n, n, n), dtype=real, device="cuda", generator=g)
+
+    def step(psi):
+        torch.mul(psi, pot, out=psi)
+        f = torch.fft.fftn(psi)
+        f.mul_(complex(0.6, 0.8))
+        psi = torch.fft.ifftn(f)
+        torch.mul(psi, pot, out=psi)
+        if not real_time:
+            psi.div_(torch.linalg.vector_norm(psi))
+        return psi
+
+    def check(psi):
+        f = torch.fft.fftn(psi)
+        e_kin = (f.abs().square() * k2).sum()
+        rho = psi.abs().square()
+        return float(e_kin + (rho * k2).sum() + rho.square().sum())   # host read, as the rule needs
+
+    for _ in range(3):
+        psi = step(psi)
+    check(psi)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(steps):
+        psi = step(psi)
+        if check_every and (i + 1) % check_every == 0:
+            check(psi)
+    e1.record()
+    torch.cuda.synchronize()
+    del psi, pot, k2
+    return e0.elapsed_time(e1)
+
+
 def batched_leg():
     """Batched parameter sweep: 64 imaginary-time solves (grids 48^3..160^3, g
     log-uniform in [100, 5000], trap aspect ratios in [0.5, 2], complex64, dt =
@@ -518,10 +577,38 @@ def batched_leg():
     a_steps = np.array([a[0] for a in alone])
     a_diag = np.array([a[1] for a in alone])
     e_diff = float(np.max(np.abs(final[:, 4] - a_diag[:, 4]) / np.abs(a_diag[:, 4])))
+    # error against the FP64 run at the same dt for a sample (one instance per grid size):
+    # the complex128 plan from the same start for the same number of steps
+    from gpe_simulator_b200 import Plan
+    psi_err = {}
+    for n in sorted({i.n for i in insts}):
+        i = next(j for j, inst in enumerate(insts) if inst.n == n)
+        inst = insts[i]
+        ref = Plan(inst.n, inst.x, inst.k, dtype=torch.complex128, kind="imaginary", beta=inst.beta, dt=inst.dt,
+                   static_expr=inst.static_expr)
+        b = states[i].to(torch.complex128).contiguous()
+        ref.step(b, int(steps[i]))
+        d = work[i].to(torch.complex128) - b
+        psi_err[str(n)] = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(b))
+        ref.close()
+    # the reference's plain form, one solve at a time, each for the steps it needs
+    plain = {}
+    for name, dtype in (("c128", torch.complex128), ("c64", torch.complex64)):
+        ms = sum(plain_form_solve_ms(inst.n, int(k), 10, dtype) for inst, k in zip(insts, steps))
+        plain[name] = ms / 1e3
+    torch.cuda.empty_cache()
     return {"instances": len(insts), "grids": sorted({i.n for i in insts}),
             "solves_per_s": len(insts) / t_batch, "wall_s": t_batch,
             "one_at_a_time_solves_per_s": len(insts) / t_alone, "one_at_a_time_wall_s": t_alone,
-            "speedup": t_alone / t_batch, "steps_median": int(np.median(steps)), "steps_max": int(steps.max()),
+            "speedup": t_alone / t_batch,
+            "plain_form_solves_per_s": {k: len(insts) / v for k, v in plain.items()},
+            "speedup_vs_plain_form": {k: v / t_batch for k, v in plain.items()},
+            "plain_form": "the reference's per-step sequence looped from Python (cuFFT via torch.fft, "
+                          "byte-equivalent elementwise kernels, normalise every step, energy check every "
+                          "10 steps), one solve at a time for the steps each solve took; c128 as the "
+                          "reference ships, c64 for comparison; device time (a floor on its wall time)",
+            "psi_err_vs_fp64_same_dt": psi_err,
+            "steps_median": int(np.median(steps)), "steps_max": int(steps.max()),
             "same_steps_as_alone": bool(np.array_equal(steps, a_steps)),
             "E_max_rel_diff_vs_alone": e_diff, "gpu_launches": int(launches),
             "criterion": "|E_k - E_{k-10}| / (10 |E_k|) < 1e-9 or 5000 steps"}
@@ -532,35 +619,75 @@ def batched_leg():
 SERVE_MAX_ACTIVE = 8
 
 
-def serving_leg(count, rate):
-    """Serving stream (bounded sample of the 1000-request stream): seeded Poisson
-    arrivals at `rate`/s, 70% imaginary-time ground states 32^3..128^3 and 30%
-    real-time stirring segments of 500-5000 steps on 8 resident states 64^3..256^3,
-    complex64, 150 GB budget; the continuous-batching server against the plain
-    one-at-a-time path on the same stream.  Results must be identical."""
+def serving_leg(count, rates, plain_sample):
+    """Serving stream (config 5): ``count`` requests with seeded Poisson arrivals at
+    each rate of ``rates``; 70% imaginary-time ground states 32^3..128^3 and 30%
+    real-time stirring segments of 500-5000 steps on 8 resident states
+    64^3..256^3, complex64, 150 GB budget and the device's free memory.  The
+    continuous-batching server against one request at a time through single
+    plans on the same stream (results must be identical), and, on the first
+    ``plain_sample`` requests, against the reference's plain form one request at
+    a time (its per-step sequence for the steps each request took; service time
+    only, no arrival gaps, so an upper bound on its throughput)."""
     import torch
     from gpe_simulator_b200 import serve
-    reqs = serve.workload(count, rate=rate, seed=2)
-    sess = serve.make_sessions()
-    t0 = time.perf_counter()
-    serve.Server(sess, budget=150e9, max_active=SERVE_MAX_ACTIVE).run(reqs)
-    wall = time.perf_counter() - t0
-    mixed = serve.summarise(reqs)
-    reqs2 = serve.workload(count, rate=rate, seed=2)
-    sess2 = serve.make_sessions()
-    serve.run_plain(reqs2, sess2)
-    plain = serve.summarise(reqs2)
-    same = all(a.taken == b.taken and (a.kind != "imaginary" or torch.equal(a.result["psi"], b.result["psi"]))
-               for a, b in zip(reqs, reqs2))
-    same = same and all(torch.equal(x.psi, y.psi) for x, y in zip(sess, sess2))
-    out = {"requests": count, "rate_per_s": rate, "imaginary": sum(r.kind == "imaginary" for r in reqs),
-           "max_active_solves": SERVE_MAX_ACTIVE,
-           "solves_per_s": mixed["solves_per_s"], "p50_ms": mixed["p50_ms"], "p99_ms": mixed["p99_ms"],
-           "plain_solves_per_s": plain["solves_per_s"], "plain_p50_ms": plain["p50_ms"],
-           "plain_p99_ms": plain["p99_ms"], "speedup": mixed["solves_per_s"] / plain["solves_per_s"],
-           "results_identical_to_plain": bool(same), "wall_s": wall}
-    for s_ in sess + sess2:
-        s_.plan.close()
+    out = {"requests": count, "max_active_solves": SERVE_MAX_ACTIVE, "budget_bytes": 150e9, "rates": []}
+    first = None
+    for rate in rates:
+        reqs = serve.workload(count, rate=rate, seed=2)
+        sess = serve.make_sessions()
+        srv = serve.Server(sess, budget=150e9, max_active=SERVE_MAX_ACTIVE)
+        t0 = time.perf_counter()
+        srv.run(reqs)
+        wall = time.perf_counter() - t0
+        mixed = serve.summarise(reqs)
+        reqs2 = serve.workload(count, rate=rate, seed=2)
+        sess2 = serve.make_sessions()
+        serve.run_plain(reqs2, sess2)
+        plain = serve.summarise(reqs2)
+        same = all(a.taken == b.taken and (a.kind != "imaginary" or torch.equal(a.result["psi"], b.result["psi"]))
+                   for a, b in zip(reqs, reqs2))
+        same = same and all(torch.equal(x.psi, y.psi) for x, y in zip(sess, sess2))
+        out["rates"].append({
+            "rate_per_s": rate, "imaginary": sum(r.kind == "imaginary" for r in reqs),
+            "solves_per_s": mixed["solves_per_s"], "p50_ms": mixed["p50_ms"], "p99_ms": mixed["p99_ms"],
+            "makespan_s": mixed["makespan_s"], "one_at_a_time_solves_per_s": plain["solves_per_s"],
+            "one_at_a_time_p50_ms": plain["p50_ms"], "one_at_a_time_p99_ms": plain["p99_ms"],
+            "speedup": mixed["solves_per_s"] / plain["solves_per_s"],
+            "admissions_deferred_for_memory": srv.refused,
+            "results_identical_to_one_at_a_time": bool(same), "wall_s": wall})
+        if first is None:
+            first = reqs
+        for s_ in sess + sess2:
+            s_.plan.close()
+        del reqs2
+        torch.cuda.empty_cache()
+    # the reference's plain form on a sample of the stream, one request at a time
+    sample = sorted(first, key=lambda r: r.arrival)[:plain_sample]
+    grids = dict(enumerate(n for n, _ in serve.SESSION_GRIDS))
+    plain_form = {}
+    for name, dtype in (("c128", torch.complex128), ("c64", torch.complex64)):
+        ms = 0.0
+        for r in sample:
+            if r.kind == "imaginary":
+                ms += plain_form_solve_ms(r.inst.n, r.taken, 20, dtype)
+            else:
+                ms += plain_form_solve_ms(grids[r.session], r.taken, 0, dtype, real_time=True)
+        plain_form[name] = len(sample) / (ms / 1e3)
+    torch.cuda.empty_cache()
+    top = max(out["rates"], key=lambda d: d["solves_per_s"])
+    out["plain_form_sample_requests"] = len(sample)
+    out["plain_form_solves_per_s"] = plain_form
+    out["speedup_vs_plain_form"] = {k: top["solves_per_s"] / v for k, v in plain_form.items()}
+    out["plain_form"] = ("the reference's per-step sequence (cuFFT via torch.fft, byte-equivalent "
+                         "elementwise kernels, normalise every imaginary step, energy check every 20 "
+                         "steps) one request at a time for the steps each request took, device time "
+                         "without arrival gaps; compared with the server's solves/s at its best rate")
+    # headline keys of the first rate
+    out.update({k: out["rates"][0][k] for k in ("rate_per_s", "solves_per_s", "p50_ms", "p99_ms",
+                                                 "one_at_a_time_solves_per_s", "one_at_a_time_p50_ms",
+                                                 "one_at_a_time_p99_ms", "speedup",
+                                                 "results_identical_to_one_at_a_time")})
     return out
 
 
@@ -624,8 +751,11 @@ def main():
                     help="sweep path of the main leg: default, tma (y/x pencils staged by TMA), "
                          "plane (y/z sweeps fused per x-plane), auto (timed once per device and "
                          "cached); identical results")
-    ap.add_argument("--serve-requests", type=int, default=120)
-    ap.add_argument("--serve-rate", type=float, default=50.0)
+    ap.add_argument("--serve-requests", type=int, default=1000, help="requests of the serving stream")
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[50.0],
+                    help="Poisson arrival rates (requests/s) of the serving stream")
+    ap.add_argument("--serve-plain-sample", type=int, default=100,
+                    help="requests of the stream also run in the reference's plain form")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -1,11 +1,15 @@
-"""Batched imaginary-time ground-state solves of mixed grid sizes.
+"""Batched solves of mixed grid sizes: imaginary-time ground states and
+real-time stirred evolutions.
 
-Many independent solves (sweeps over g, trap aspect ratios and grid sizes)
-advance together: ``gpe_batch_*`` groups the instances by grid size, launches
-every sweep once per group over (tiles x instances), and replays one step of
-all groups from a CUDA graph with a parallel branch per group.  Each instance
-runs exactly the arithmetic of its own single-plan step, so a solve gives the
-same bits alone and in the batch.
+Many independent solves (sweeps over g, trap aspect ratios, grid sizes and
+stirring rates) advance together: ``gpe_batch_*`` groups the instances by grid
+size and kind, launches every sweep once per group over (tiles x instances),
+and replays one step of all groups from a CUDA graph with a parallel branch
+per group.  Each instance runs exactly the arithmetic of its own single-plan
+one-step call, so a solve gives the same bits alone and in the batch.
+Real-time instances keep a clock (steps taken); each step evaluates the
+stirring beam at ``t_mid = step * dt + dt/2`` as ``gpe/launch.py:10`` and
+``gpe/make_propagator.py:94`` do.
 
 :func:`solve` runs every instance until ``|E_k - E_{k-K}| / (K |E_k|) < tol``
 (energy change per step, checked every ``K`` steps) or ``max_steps``, retiring
@@ -26,13 +30,17 @@ from .plan import _DTYPES, _dptr, _stream
 
 @dataclass
 class Instance:
-    """One solve, in reference units (kinetic factor ``exp(-i c k^2 dt)``)."""
+    """One solve, in reference units (kinetic factor ``exp(-i c k^2 dt)``):
+    ``kind`` ``"imaginary"`` (ground state) or ``"real"`` (stirred evolution with
+    the built-in ``beam``, a :class:`~gpe_simulator_b200.plan.Beam`)."""
     n: int
     simulation_range: float
     beta: float
     dt: float
     static_expr: str = "0"
     kinetic_coeff: float = 1.0
+    kind: str = "imaginary"
+    beam: object = None
     x: np.ndarray = field(init=False, repr=False)
     k: np.ndarray = field(init=False, repr=False)
 
@@ -43,7 +51,17 @@ class Instance:
 
 
 def _fill_desc(d, inst, dtype, keep):
-    d.n, d.dtype, d.kind = inst.n, _DTYPES[dtype], _lib.IMAGINARY
+    if inst.kind not in ("imaginary", "real"):
+        raise KeyError("kind must be 'imaginary' or 'real'")
+    d.n, d.dtype = inst.n, _DTYPES[dtype]
+    d.kind = _lib.IMAGINARY if inst.kind == "imaginary" else _lib.REAL
+    if inst.beam is not None:
+        if inst.kind != "real":
+            raise ValueError("Imaginary time evolution does not accept a time dependent potential.")
+        b = inst.beam
+        d.beam_enabled = 1
+        d.beam_amp, d.beam_width, d.beam_radius, d.beam_omega, d.beam_t_ramp = (
+            float(b.amp), float(b.width), float(b.radius), float(b.omega), float(b.t_ramp))
     d.beta, d.dt, d.kinetic_coeff = float(inst.beta), float(inst.dt), float(inst.kinetic_coeff)
     a, d.x_array = _dptr(inst.x)
     keep.append(a)
@@ -139,6 +157,16 @@ class Batch:
             self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream()))
         return out
 
+    def set_step(self, index, step):
+        """Clock of real-time instance ``index``: steps taken (its next step evaluates
+        the beam at ``step * dt + dt/2``)."""
+        _lib.check(self.lib.gpe_batch_set_step(self._h, int(index), int(step)))
+
+    def get_step(self, index):
+        out = ctypes.c_longlong()
+        _lib.check(self.lib.gpe_batch_get_step(self._h, int(index), ctypes.byref(out)))
+        return out.value
+
     def launch_count(self):
         out = ctypes.c_longlong()
         _lib.check(self.lib.gpe_batch_launch_count(self._h, ctypes.byref(out)))
@@ -217,6 +245,24 @@ def sweep_instances(count=64, seed=1, dt=1e-3):
         ly, lz = rng.uniform(0.5, 2.0, 2)
         expr = f"x**2+{float(ly * ly)!r}*y**2+{float(lz * lz)!r}*z**2"
         out.append(Instance(n=n, simulation_range=2 * L, beta=2 * g, dt=dt / 2, static_expr=expr))
+    return out
+
+
+def stirring_instances(rates=(0.25, 0.5, 1.0), gs=(500.0, 1000.0), grids=((64, 16.0), (96, 20.0)),
+                       dt=5e-4):
+    """A stirring-rate sweep, in reference units: for every grid (side, box length),
+    interaction g and final angular rate Omega of the beam (oscillator units A = 10,
+    w = 0.5, R = 2, rate ramped 0 -> Omega over 200 steps), the trap
+    V = (x^2 + 1.44 y^2 + 2.25 z^2)/2 with oscillator time step ``dt``.  Mapped
+    exactly onto the reference convention: V x2, g x2, dt/2, rates x2."""
+    from .plan import beam_in_reference_units
+    out = []
+    for n, L in grids:
+        for g in gs:
+            for omega in rates:
+                beam = beam_in_reference_units(10.0, 0.5, 2.0, omega, 200 * dt)
+                out.append(Instance(n=n, simulation_range=L, beta=2 * g, dt=dt / 2,
+                                    static_expr="x**2+1.44*y**2+2.25*z**2", kind="real", beam=beam))
     return out
 
 

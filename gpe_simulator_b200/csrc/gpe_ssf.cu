@@ -405,6 +405,26 @@ struct DiagJob {
   int na, nb, index;
 };
 
+// Real-time batch groups: member q takes entry tick[q] of the call's time table
+// (host-computed, FP64: t_mid of the step and the beam centres at it, t at the
+// step's end and the centres there) into its z sweeps' and diagnostics'
+// descriptors, then advances.
+__global__ void k_batch_clock(Sweep* sws, int m, const double* times, int* tick, int r1, int r2, int rd) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= m) return;
+  const double* e = times + ((size_t)tick[q] * m + q) * 6;
+  Sweep* a = sws + (size_t)r1 * m + q;
+  Sweep* b = sws + (size_t)r2 * m + q;
+  Sweep* d = sws + (size_t)rd * m + q;
+  a->t1 = b->t1 = e[0];
+  a->bc1x = b->bc1x = e[1];
+  a->bc1y = b->bc1y = e[2];
+  d->t1 = e[3];
+  d->bc1x = e[4];
+  d->bc1y = e[5];
+  tick[q] += 1;
+}
+
 __global__ void k_finish_diag_batch(const DiagJob* jobs, double* out) {
   __shared__ Acc sh[32 * 4];
   const DiagJob j = jobs[blockIdx.x];
@@ -1622,6 +1642,7 @@ struct gpe_batch {
   std::vector<gpe_plan*> plans;
   struct Group {
     int n = 0;
+    int kind = GPE_IMAGINARY;   // real-time groups: no renormalisation, per-step clock
     bool fast = false;
     std::vector<int> all;       // every instance of this size
     std::vector<int> members;   // the bound (active) ones
@@ -1631,9 +1652,16 @@ struct gpe_batch {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
     int uploaded = 0;           // member count the device arrays hold
+    // real time: half-step time and beam centres of every step of the current call,
+    // [step][member][6] = {t_mid, cx, cy, t_end, cx, cy}, and each member's position in it
+    double* d_times = nullptr;
+    double* h_times = nullptr;  // pinned staging of the same
+    int* d_tick = nullptr;
+    int times_cap = 0;          // members the arrays hold (for BATCH_CLOCK_STEPS steps)
   };
   std::vector<Group> groups;
   std::vector<void*> psis;
+  std::vector<long long> clock;   // real time: steps taken by each instance (t = clock * dt)
   cudaGraphExec_t graph = nullptr;
   cudaGraph_t graph_def = nullptr;
   cudaEvent_t fork = nullptr;
@@ -1651,6 +1679,60 @@ namespace {
 
 enum { ROLE_Z1N = 0, ROLE_Z1, ROLE_Y1, ROLE_X, ROLE_Y2, ROLE_Z2, ROLE_SC, ROLE_DZ, ROLE_DY, ROLE_DX, ROLE_COUNT };
 
+// steps of a real-time group's time table per upload (longer calls are chunked)
+constexpr int BATCH_CLOCK_STEPS = 1024;
+
+// Group of (grid size, kind), created on first use.
+int batch_group(gpe_batch* b, const gpe_plan* p, bool make_streams) {
+  for (size_t q = 0; q < b->groups.size(); ++q)
+    if (b->groups[q].n == p->n && b->groups[q].kind == p->kind) return (int)q;
+  gpe_batch::Group g;
+  g.n = p->n;
+  g.kind = p->kind;
+  g.fast = p->fast;
+  if (make_streams) {
+    if (cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    if (cudaEventCreateWithFlags(&g.ev, cudaEventDisableTiming) != cudaSuccess) return -1;
+  }
+  b->groups.push_back(g);
+  return (int)b->groups.size() - 1;
+}
+
+// What a batch instance may be: imaginary time, or real time with the built-in
+// stirring beam (dynamic expressions need the per-launch line table of a plan).
+int batch_check_desc(const gpe_batch* b, const gpe_desc* d) {
+  if (d->kind != GPE_IMAGINARY && d->kind != GPE_REAL) return fail(GPE_ERR_ARG, "kind must be imaginary or real");
+  if (d->kind == GPE_REAL && d->dynamic_g_len)
+    return fail(GPE_ERR_ARG, "batched real-time instances take the built-in beam, not dynamic expressions");
+  if (d->dtype != b->dtype) return fail(GPE_ERR_ARG, "all instances of a batch share one dtype");
+  return GPE_OK;
+}
+
+// Fill and upload the time tables of every bound real-time group for steps
+// [first, first + count) of the call (count <= BATCH_CLOCK_STEPS).
+int batch_times(gpe_batch* b, long long first, int count, cudaStream_t st) {
+  for (auto& g : b->groups) {
+    if (g.kind != GPE_REAL || g.members.empty()) continue;
+    const int m = (int)g.members.size();
+    for (int q = 0; q < m; ++q) {
+      const gpe_plan* p = b->plans[g.members[q]];
+      const long long s0 = b->clock[g.members[q]] + first;
+      for (int k = 0; k < count; ++k) {
+        Sweep a;
+        a.t1 = t_mid_host(p, s0 + k);              // gpe/launch.py:10 + gpe/make_propagator.py:94
+        a.t2 = (double)(s0 + k + 1) * p->dt;       // the state's time after the step
+        beam_centres(p, a);
+        double* e = g.h_times + ((size_t)k * m + q) * 6;
+        e[0] = a.t1; e[1] = a.bc1x; e[2] = a.bc1y;
+        e[3] = a.t2; e[4] = a.bc2x; e[5] = a.bc2y;
+      }
+    }
+    CU(cudaMemcpyAsync(g.d_times, g.h_times, sizeof(double) * 6 * (size_t)m * count, cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(g.d_tick, 0, sizeof(int) * m, st));
+  }
+  return GPE_OK;
+}
+
 void batch_free_graph(gpe_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->graph_def) cudaGraphDestroy(b->graph_def);
@@ -1663,6 +1745,9 @@ void batch_free(gpe_batch* b) {
   for (auto& g : b->groups) {
     if (g.d_ph) cudaFree(g.d_ph);
     if (g.d_sw) cudaFree(g.d_sw);
+    if (g.d_times) cudaFree(g.d_times);
+    if (g.d_tick) cudaFree(g.d_tick);
+    if (g.h_times) cudaFreeHost(g.h_times);
     if (g.stream) cudaStreamDestroy(g.stream);
     if (g.ev) cudaEventDestroy(g.ev);
   }
@@ -1688,7 +1773,11 @@ Sweep role_sweep(int role, void* psi, gpe_plan* p) {
     case ROLE_Y1: s.fft1 = 1; break;
     case ROLE_X: s.fft1 = 1; s.mid = PW_KIN | PW_CONJ_LAST; s.fft2 = 1; s.post = PW_CONJ_FIRST; break;
     case ROLE_Y2: s.pre = PW_CONJ_LAST; s.fft1 = 1; s.post = PW_CONJ_FIRST; break;
-    case ROLE_Z2: s.pre = PW_CONJ_LAST; s.fft1 = 1; s.post = PW_CONJ_FIRST | PW_INVM | PW_HALF1 | PW_NORM; break;
+    case ROLE_Z2:
+      s.pre = PW_CONJ_LAST;
+      s.fft1 = 1;
+      s.post = PW_CONJ_FIRST | PW_INVM | PW_HALF1 | (p->kind == GPE_IMAGINARY ? PW_NORM : 0u);
+      break;
     case ROLE_SC: s.pre = PW_SCALE; break;
     // diagnostics: real-space sums + forward z/y into the work buffer, k-space sums in x
     case ROLE_DZ: s.dst = p->d_work; s.pre = PW_DIAG_R; s.fft1 = 1; s.t1 = 0.0; break;
@@ -1735,7 +1824,7 @@ int group_launch(gpe_batch* b, gpe_batch::Group& g, int role, cudaStream_t st) {
       case ROLE_DZ: op = mk_ops(FM_DIAGR); break;
       case ROLE_DY: op = mk_ops(FM_PLAIN); break;
       case ROLE_DX: op = mk_ops(FM_DIAGK); break;
-      default: op = mk_ops(FM_Z2, 0, 0, 0, 1); break;
+      default: op = mk_ops(FM_Z2, 0, 0, 0, g.kind == GPE_IMAGINARY ? 1 : 0); break;
     }
     CU(launch_fast_batch<R>(g.n, fax, g.d_ph, sws, count, op, st));
   } else {
@@ -1755,6 +1844,19 @@ int group_role(gpe_batch* b, gpe_batch::Group& g, int role, cudaStream_t st) {
 }
 
 int group_step(gpe_batch* b, gpe_batch::Group& g, bool scaled, cudaStream_t st) {
+  if (g.kind == GPE_REAL) {
+    // this step's half-step time and beam centres into the z sweeps' (and the
+    // diagnostics') sweep descriptors
+    const int m = (int)g.members.size();
+    k_batch_clock<<<(m + 127) / 128, 128, 0, st>>>(g.d_sw, m, g.d_times, g.d_tick, ROLE_Z1N, ROLE_Z2, ROLE_DZ);
+    CU(cudaGetLastError());
+    ++b->launches;
+    TRY(group_role(b, g, ROLE_Z1N, st));
+    TRY(group_role(b, g, ROLE_Y1, st));
+    TRY(group_role(b, g, ROLE_X, st));
+    TRY(group_role(b, g, ROLE_Y2, st));
+    return group_role(b, g, ROLE_Z2, st);
+  }
   TRY(group_role(b, g, scaled ? ROLE_Z1 : ROLE_Z1N, st));
   TRY(group_role(b, g, ROLE_Y1, st));
   TRY(group_role(b, g, ROLE_X, st));
@@ -1790,6 +1892,19 @@ int group_upload(gpe_batch* b, gpe_batch::Group& g) {
     CU(cudaMalloc(&g.d_sw, sizeof(Sweep) * m * ROLE_COUNT));
     g.cap = m;
   }
+  if (g.kind == GPE_REAL && m > g.times_cap) {
+    if (g.d_times) cudaFree(g.d_times);
+    if (g.d_tick) cudaFree(g.d_tick);
+    if (g.h_times) cudaFreeHost(g.h_times);
+    g.d_times = nullptr;
+    g.d_tick = nullptr;
+    g.h_times = nullptr;
+    const size_t bytes = sizeof(double) * 6 * (size_t)m * BATCH_CLOCK_STEPS;
+    CU(cudaMalloc(&g.d_times, bytes));
+    CU(cudaMallocHost(&g.h_times, bytes));
+    CU(cudaMalloc(&g.d_tick, sizeof(int) * m));
+    g.times_cap = m;
+  }
   std::vector<Phys> hph(m);
   std::vector<Sweep> hsw((size_t)m * ROLE_COUNT);
   for (int q = 0; q < m; ++q) {
@@ -1799,6 +1914,11 @@ int group_upload(gpe_batch* b, gpe_batch::Group& g) {
     hph[q] = p->ph;
     for (int role = 0; role < ROLE_COUNT; ++role) {
       Sweep s = role_sweep(role, b->psis[g.members[q]], p);
+      if (g.kind == GPE_REAL && role == ROLE_DZ) {
+        // diagnostics at the instance's current time (the clock kernel keeps it current)
+        s.t1 = s.t2 = (double)b->clock[g.members[q]] * p->dt;
+        beam_centres(p, s);
+      }
       int tiles = 0, threads = 0;
       size_t smem = 0;
       const int rc = b->dtype == GPE_C64 ? sweep_geometry<float>(p, role_axis(role), s, tiles, threads, smem)
@@ -1857,24 +1977,15 @@ int gpe_batch_create(const gpe_desc* descs, int count, gpe_batch** out) {
   gpe_batch* b = new gpe_batch();
   b->dtype = count > 0 ? descs[0].dtype : GPE_C64;
   for (int i = 0; i < count; ++i) {
-    if (descs[i].kind != GPE_IMAGINARY) { batch_free(b); return fail(GPE_ERR_ARG, "batches hold imaginary-time solves"); }
-    if (descs[i].dtype != b->dtype) { batch_free(b); return fail(GPE_ERR_ARG, "all instances of a batch share one dtype"); }
+    int rc = batch_check_desc(b, &descs[i]);
+    if (rc != GPE_OK) { batch_free(b); return rc; }
     gpe_plan* p = nullptr;
-    const int rc = create(&descs[i], &p);
+    rc = create(&descs[i], &p);
     if (rc != GPE_OK) { batch_free(b); return rc; }
     b->plans.push_back(p);
-    int gi = -1;
-    for (size_t q = 0; q < b->groups.size(); ++q)
-      if (b->groups[q].n == p->n) gi = (int)q;
-    if (gi < 0) {
-      gpe_batch::Group g;
-      g.n = p->n;
-      g.fast = p->fast;
-      b->groups.push_back(g);
-      gi = (int)b->groups.size() - 1;
-    }
-    b->groups[gi].all.push_back(i);
+    b->groups[batch_group(b, p, false)].all.push_back(i);
   }
+  b->clock.assign(count, 0);
   for (auto& g : b->groups) {
     CU(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     CU(cudaEventCreateWithFlags(&g.ev, cudaEventDisableTiming));
@@ -1890,8 +2001,7 @@ int gpe_batch_create(const gpe_desc* descs, int count, gpe_batch** out) {
 
 int gpe_batch_add(gpe_batch* b, const gpe_desc* d, int* index) {
   if (!b || !d || !index) return fail(GPE_ERR_ARG, "null argument");
-  if (d->kind != GPE_IMAGINARY) return fail(GPE_ERR_ARG, "batches hold imaginary-time solves");
-  if (d->dtype != b->dtype) return fail(GPE_ERR_ARG, "all instances of a batch share one dtype");
+  TRY(batch_check_desc(b, d));
   gpe_plan* p = nullptr;
   TRY(create(d, &p));
   int slot = -1;
@@ -1901,6 +2011,7 @@ int gpe_batch_add(gpe_batch* b, const gpe_desc* d, int* index) {
     slot = (int)b->plans.size();
     b->plans.push_back(nullptr);
     b->psis.push_back(nullptr);
+    b->clock.push_back(0);
     double* h = nullptr;
     CU(cudaMallocHost(&h, sizeof(double) * 4 * b->plans.size()));
     if (b->h_sums) cudaFreeHost(b->h_sums);
@@ -1908,18 +2019,9 @@ int gpe_batch_add(gpe_batch* b, const gpe_desc* d, int* index) {
   }
   b->plans[slot] = p;
   b->psis[slot] = nullptr;
-  int gi = -1;
-  for (size_t q = 0; q < b->groups.size(); ++q)
-    if (b->groups[q].n == p->n) gi = (int)q;
-  if (gi < 0) {
-    gpe_batch::Group g;
-    g.n = p->n;
-    g.fast = p->fast;
-    CU(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
-    CU(cudaEventCreateWithFlags(&g.ev, cudaEventDisableTiming));
-    b->groups.push_back(g);
-    gi = (int)b->groups.size() - 1;
-  }
+  b->clock[slot] = 0;
+  const int gi = batch_group(b, p, true);
+  if (gi < 0) return fail(GPE_ERR_CUDA, "stream or event creation failed");
   b->groups[gi].all.push_back(slot);
   *index = slot;
   return GPE_OK;
@@ -1983,25 +2085,33 @@ int gpe_batch_step(gpe_batch* b, int nsteps, void* stream) {
   bool any = false;
   for (auto& g : b->groups) any = any || !g.members.empty();
   if (!any) return GPE_OK;
-  TRY(batch_step_all(b, false, st));  // first step: psi is normalised, no pending scale
-  if (nsteps > 1) {
-    if (!b->graph) {
-      // capture on the batch's own stream (the caller's may be the legacy default stream)
-      CU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
-      const int rc = batch_step_all(b, true, b->cap);
-      cudaGraph_t gdef = nullptr;
-      const cudaError_t e = cudaStreamEndCapture(b->cap, &gdef);
-      if (rc != GPE_OK) { if (gdef) cudaGraphDestroy(gdef); return rc; }
-      CU(e);
-      b->graph_def = gdef;
-      CU(cudaGraphInstantiate(&b->graph, gdef, 0));
-    }
-    for (int s = 1; s < nsteps; ++s) CU(cudaGraphLaunch(b->graph, st));
+  if (nsteps > 1 && !b->graph) {
+    // capture on the batch's own stream (the caller's may be the legacy default stream)
+    CU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    const int rc = batch_step_all(b, true, b->cap);
+    cudaGraph_t gdef = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->cap, &gdef);
+    if (rc != GPE_OK) { if (gdef) cudaGraphDestroy(gdef); return rc; }
+    CU(e);
+    b->graph_def = gdef;
+    CU(cudaGraphInstantiate(&b->graph, gdef, 0));
   }
-  // apply the last renormalisation
+  for (int c0 = 0; c0 < nsteps; c0 += BATCH_CLOCK_STEPS) {
+    const int count = std::min(BATCH_CLOCK_STEPS, nsteps - c0);
+    if (c0 > 0) CU(cudaStreamSynchronize(st));   // the previous table has left the staging buffer
+    TRY(batch_times(b, c0, count, st));
+    for (int s = 0; s < count; ++s) {
+      if (c0 + s == 0) TRY(batch_step_all(b, false, st));  // first step: psi is normalised, no pending scale
+      else CU(cudaGraphLaunch(b->graph, st));
+    }
+  }
+  for (auto& g : b->groups)
+    if (g.kind == GPE_REAL)
+      for (int i : g.members) b->clock[i] += nsteps;
+  // apply the last renormalisation (imaginary-time groups)
   CU(cudaEventRecord(b->fork, st));
   for (auto& g : b->groups) {
-    if (g.members.empty()) continue;
+    if (g.members.empty() || g.kind != GPE_IMAGINARY) continue;
     CU(cudaStreamWaitEvent(g.stream, b->fork, 0));
     TRY(group_role(b, g, ROLE_SC, g.stream));
     CU(cudaEventRecord(g.ev, g.stream));
@@ -2032,6 +2142,28 @@ int gpe_batch_diagnostics(gpe_batch* b, double* scalars, void* stream) {
   CU(cudaStreamSynchronize(st));
   for (auto& g : b->groups)
     for (int i : g.members) diag_scalars(b->plans[i], b->h_sums + 4 * i, scalars + 6 * i);
+  return GPE_OK;
+}
+
+int gpe_batch_set_step(gpe_batch* b, int index, long long step) {
+  if (!b || index < 0 || index >= (int)b->plans.size() || !b->plans[index])
+    return fail(GPE_ERR_ARG, "no such batch instance");
+  if (b->plans[index]->kind != GPE_REAL) return fail(GPE_ERR_ARG, "only real-time instances have a clock");
+  if (step < 0) return fail(GPE_ERR_ARG, "step must be >= 0");
+  for (auto& g : b->groups) CU(cudaStreamSynchronize(g.stream));
+  b->clock[index] = step;
+  for (auto& g : b->groups)
+    if (std::find(g.members.begin(), g.members.end(), index) != g.members.end()) {
+      batch_free_graph(b);
+      TRY(group_upload(b, g));
+    }
+  return GPE_OK;
+}
+
+int gpe_batch_get_step(const gpe_batch* b, int index, long long* step) {
+  if (!b || !step || index < 0 || index >= (int)b->plans.size() || !b->plans[index])
+    return fail(GPE_ERR_ARG, "no such batch instance");
+  *step = b->clock[index];
   return GPE_OK;
 }
 

@@ -4,7 +4,8 @@ Requests arrive over time (seeded Poisson process).  Each scheduling round the
 server
 
 1. admits every request that has arrived, while the device memory it needs fits
-   the HBM budget (requests wait in arrival order otherwise);
+   both the HBM budget and the memory the device reports free (queried every
+   round; requests wait in arrival order otherwise);
 2. advances all admitted work by one chunk: the imaginary-time solves as one
    running :class:`Batch` (instances added on admission, removed on
    convergence), and every real-time segment on its own CUDA stream, so the
@@ -117,11 +118,17 @@ class Server:
     """Continuous batching over a running imaginary-time :class:`Batch` and
     real-time segments on per-session streams (see the module docstring)."""
 
-    def __init__(self, sessions, dtype=torch.complex64, budget=150e9, chunk=20, max_active=None):
+    def __init__(self, sessions, dtype=torch.complex64, budget=150e9, chunk=20, max_active=None,
+                 mem_info=None, reserve=2 << 30):
         self.sessions = sessions
         self.dtype = dtype
         self.budget = budget
         self.chunk = chunk
+        # (free, total) bytes of the device; admission keeps `reserve` bytes free for
+        # the allocator's own blocks and the plans' tables
+        self.mem_info = mem_info or torch.cuda.mem_get_info
+        self.reserve = reserve
+        self.refused = 0       # admissions deferred because the device lacked free memory
         # at most this many imaginary-time solves advance together (None: as many as
         # the memory budget admits); fewer finish sooner, more share each launch
         self.max_active = max_active
@@ -143,9 +150,12 @@ class Server:
             now = clock()
             while pending and pending[0].arrival <= now:
                 queue.append(pending.pop(0))
-            # admission in arrival order: memory budget for solves, a free session for segments
+            # admission in arrival order: the memory budget and the device's free memory
+            # for solves, a free session for segments
             changed = False
             keep = []
+            free = self.mem_info()[0] - self.reserve if queue else 0
+            short = None   # a solve the device's free memory could not take this round
             for r in queue:
                 if r.kind == "imaginary":
                     need = state_bytes(r.inst.n, self.dtype)
@@ -153,6 +163,12 @@ class Server:
                     if used + need > self.budget or full:
                         keep.append(r)
                         continue
+                    if need > free:
+                        self.refused += 1
+                        short = short or (r, need)
+                        keep.append(r)
+                        continue
+                    free -= need
                     with torch.cuda.stream(self.batch_stream):
                         idx = batch.add(r.inst)
                         psi = initial_states([r.inst], self.dtype, seed0=10_000 + r.rid)[0]
@@ -173,6 +189,11 @@ class Server:
                     sess.step += r.steps
                     real[r.session] = (r, ev)
             queue = keep
+            if short and not imag and not real:
+                # nothing of ours is running to free memory: waiting would not end
+                r, need = short
+                raise MemoryError(f"request {r.rid} needs {need} bytes of device memory; the device has "
+                                  f"{max(free, 0)} free beyond the {self.reserve}-byte reserve")
             if imag:
                 with torch.cuda.stream(self.batch_stream):
                     if changed:

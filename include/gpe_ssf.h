@@ -198,20 +198,28 @@ int  gpe_profile_read(gpe_plan* plan, double* ms, long long* count);
  * shared-memory layout (its tiles were not transformed); read and clear (synchronises) */
 int  gpe_status(gpe_plan* plan, int* flags, void* stream);
 
-/* Batches: many independent imaginary-time solves (mixed grid sizes, one dtype)
- * advanced together.  Instances are grouped by grid size; each sweep is one
- * launch per group over (tiles x instances), and one step of all groups is
- * replayed from a CUDA graph with a parallel branch per group.  Replaces calling
- * standard_imaginary_step (gpe/make_propagator.py:109-151) for each solve in turn.
+/* Batches: many independent solves (mixed grid sizes, one dtype) advanced together:
+ * imaginary-time ground states, and real-time stirred evolutions with the built-in
+ * beam (a stirring-rate sweep).  Instances are grouped by grid size and kind; each
+ * sweep is one launch per group over (tiles x instances), and one step of all
+ * groups is replayed from a CUDA graph with a parallel branch per group.  Replaces
+ * calling standard_imaginary_step (gpe/make_propagator.py:109-151) or
+ * time_dependent_propagator (:57-103) for each solve in turn.  Every instance
+ * computes the arithmetic of its own plan's one-step call (gpe_step with
+ * nsteps = 1), so results are identical alone and batched.
  *   gpe_batch_create: count >= 0 instances (an empty batch takes its dtype from
- *     the first gpe_batch_add when count = 0 -- complex64 otherwise).
+ *     the first gpe_batch_add when count = 0 -- complex64 otherwise).  Real-time
+ *     instances take no dynamic expression (the built-in beam only).
  *   gpe_batch_add / gpe_batch_remove: grow or shrink a running batch (continuous
  *     batching); add returns the new instance's index (a freed index is reused).
  *   gpe_batch_bind: psi pointers of every instance (device, C-contiguous) and an
  *     optional active mask (NULL = all); rebinding discards the captured graph.
- *   gpe_batch_step: nsteps renormalised steps of every bound instance.
+ *   gpe_batch_step: nsteps steps of every bound instance (imaginary time
+ *     renormalised every step; real time at t = step * dt of each instance's clock).
+ *   gpe_batch_set_step / gpe_batch_get_step: a real-time instance's clock (steps
+ *     taken; its next step evaluates the beam at t_mid = step * dt + dt/2).
  *   gpe_batch_diagnostics: scalars[6*i .. 6*i+5] = {N, E_kin, E_pot, E_int, E, mu}
- *     of every bound instance i (synchronises). */
+ *     of every bound instance i (synchronises); real-time instances at their clock's t. */
 typedef struct gpe_batch gpe_batch;
 int  gpe_batch_create(const gpe_desc* descs, int count, gpe_batch** batch);
 int  gpe_batch_destroy(gpe_batch* batch);
@@ -220,6 +228,8 @@ int  gpe_batch_remove(gpe_batch* batch, int index);
 int  gpe_batch_bind(gpe_batch* batch, void* const* psis, const int* active, void* stream);
 int  gpe_batch_step(gpe_batch* batch, int nsteps, void* stream);
 int  gpe_batch_diagnostics(gpe_batch* batch, double* scalars, void* stream);
+int  gpe_batch_set_step(gpe_batch* batch, int index, long long step);
+int  gpe_batch_get_step(const gpe_batch* batch, int index, long long* step);
 int  gpe_batch_launch_count(const gpe_batch* batch, long long* count);
 
 /* Renormalise psi in place (psi /= sqrt(N), N = dx^3 sum |psi|^2) without allocating

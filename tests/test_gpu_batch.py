@@ -150,3 +150,62 @@ def test_serving_matches_one_at_a_time(cuda):
         assert torch.equal(x.psi, y.psi)
     summary = serve.summarise(reqs)
     assert summary["requests"] == 24 and summary["p99_ms"] >= summary["p50_ms"] > 0
+
+
+def test_serving_admits_by_free_device_memory(cuda):
+    """Admission consults the device's free memory every round (a fake reading,
+    injected on the host): with none free and nothing of its own running the
+    server raises instead of waiting for ever; with room for one solve per round
+    it defers the rest and still finishes every request."""
+    from gpe_simulator_b200 import serve
+
+    def solves():
+        out = [r for r in serve.workload(12, rate=1000.0, seed=3) if r.kind == "imaginary"][:4]
+        for r in out:
+            r.arrival = 0.0          # all queued at once: one admission round sees them all
+        return out
+
+    total = 180 << 30
+    with pytest.raises(MemoryError, match="free"):
+        serve.Server([], mem_info=lambda: (0, total)).run(solves())
+    one = serve.state_bytes(128, torch.complex64) + 1024
+    srv = serve.Server([], mem_info=lambda: ((1 << 30) + one, total), reserve=1 << 30)
+    reqs = solves()
+    srv.run(reqs)
+    assert srv.refused > 0
+    assert all(r.done_at is not None and r.taken > 0 for r in reqs)
+
+
+def test_real_time_stirring_sweep_batched_equals_alone_bitwise(cuda):
+    """A stirring-rate sweep (rates 0.25/0.5/1 at two grid sizes and two g) batched
+    with imaginary-time solves: every real-time state equals its own plan's
+    one-step calls bit for bit, the clock carries the beam's time, and the
+    diagnostics use the instance's current time."""
+    from gpe_simulator_b200 import Plan
+    from gpe_simulator_b200.batch import Batch, initial_states, stirring_instances, sweep_instances
+    real = stirring_instances(rates=(0.25, 0.5, 1.0), gs=(500.0, 1000.0), grids=((32, 12.0), (64, 16.0)))
+    imag = sweep_instances(3, seed=5)
+    insts = real + imag
+    states = initial_states(insts, torch.complex64, seed0=300)
+    batch = Batch(insts, torch.complex64)
+    work = [s.clone() for s in states]
+    batch.bind(work)
+    batch.set_step(1, 7)          # one instance starts further along its ramp
+    batch.step(25)
+    assert batch.get_step(1) == 32 and batch.get_step(0) == 25
+    diag = batch.diagnostics()
+    for i, inst in enumerate(insts):
+        plan = Plan(inst.n, inst.x, inst.k, dtype=torch.complex64, kind=inst.kind, beta=inst.beta, dt=inst.dt,
+                    static_expr=inst.static_expr, beam=inst.beam)
+        alone = states[i].clone()
+        s0 = 7 if i == 1 else 0
+        if inst.kind == "real":
+            for s in range(25):
+                plan.step(alone, 1, s0 + s)      # one-step calls, as the batch runs them
+        else:
+            plan.step(alone, 25)
+        assert torch.equal(alone, work[i]), (i, inst.kind, inst.n)
+        d = plan.diagnostics(alone, t=(s0 + 25) * inst.dt if inst.kind == "real" else 0.0)
+        assert np.allclose([d["N"], d["E"], d["mu"]], diag[i, [0, 4, 5]], rtol=1e-12, atol=0), i
+        plan.close()
+    batch.close()
