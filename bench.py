@@ -338,7 +338,7 @@ def ours(args, world, rank, local):
     if world == 1 and not args.no_batch:
         result["batched"] = batched_leg()
     if world == 1 and not args.no_serve:
-        result["serving"] = serving_leg(args.serve_requests, args.serve_rates, args.serve_plain_sample)
+        result["serving"] = serving_leg(args.serve_requests, args.serve_rates, args.serve_measure_one_at_a_time)
     return result, plan
 
 
@@ -490,19 +490,18 @@ def plain_floor_leg(steps=50, warmup=5):
     return out
 
 
-def plain_form_solve_ms(n, steps, check_every, dtype, real_time=False):
-    """Device milliseconds of one solve in the reference's plain form on this GPU
-    (CuPy is not installed here, so its own code cannot run): per step, looped
-    from Python as ``gpe/launch.py:8-13`` loops, the kernel sequence of
-    ``gpe/make_propagator.py:109-151`` (``57-103`` in real time) -- half-step,
-    ``fftn``, kinetic factor, ``ifftn``, half-step, and in imaginary time the
-    two-pass norm and the division of ``gpe/helper.py:81-93`` -- plus, every
-    ``check_every`` steps, the energy check of the convergence rule (``fftn`` of
-    the state and the E_kin, E_pot, E_int sums).  cuFFT runs through torch.fft;
-    each elementwise RawKernel is one torch kernel moving the same bytes (the
-    half-step reads psi and its potential array and writes psi), so the
-    reference's own solve cannot be faster.  ``steps`` is the step count the
-    solve needs (taken from the batched run, which computes the same physics)."""
+def plain_form_costs(n, dtype, real_time=False, steps=100, checks=10):
+    """Device milliseconds per step and per energy check of the reference's plain
+    form on this GPU (CuPy is not installed here, so its own code cannot run):
+    per step, looped from Python as ``gpe/launch.py:8-13`` loops, the kernel
+    sequence of ``gpe/make_propagator.py:109-151`` (``57-103`` in real time) --
+    half-step, ``fftn``, kinetic factor, ``ifftn``, half-step, and in imaginary
+    time the two-pass norm and the division of ``gpe/helper.py:81-93``; per
+    check, the ``fftn`` of the state and the E_kin, E_pot, E_int sums read on the
+    host (the convergence rule).  cuFFT runs through torch.fft; each elementwise
+    RawKernel is one torch kernel moving the same bytes (the half-step reads psi
+    and its potential array and writes psi), so the reference's own steps cannot
+    be faster.  Times include the gaps of the Python loop."""
     import torch
     real = torch.float64 if dtype == torch.complex128 else torch.float32
     g = torch.Generator(device="cuda").manual_seed(n)
@@ -539,14 +538,25 @@ def plain_form_solve_ms(n, steps, check_every, dtype, real_time=False):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record()
-    for i in range(steps):
+    for _ in range(steps):
         psi = step(psi)
-        if check_every and (i + 1) % check_every == 0:
-            check(psi)
     e1.record()
     torch.cuda.synchronize()
+    per_step = e0.elapsed_time(e1) / steps
+    e0.record()
+    for _ in range(checks):
+        check(psi)
+    e1.record()
+    torch.cuda.synchronize()
+    per_check = e0.elapsed_time(e1) / checks
     del psi, pot, k2
-    return e0.elapsed_time(e1)
+    return per_step, per_check
+
+
+PLAIN_FORM_NOTE = ("the reference's per-step sequence looped from Python (cuFFT via torch.fft, byte-equivalent "
+                   "elementwise kernels, normalise every imaginary step, an energy check every 10 (batched) or "
+                   "20 (served) steps): device ms per step and per check measured per grid size, times each "
+                   "solve's step count; c128 as the reference ships, c64 for comparison")
 
 
 def batched_leg():
@@ -594,7 +604,8 @@ def batched_leg():
     # the reference's plain form, one solve at a time, each for the steps it needs
     plain = {}
     for name, dtype in (("c128", torch.complex128), ("c64", torch.complex64)):
-        ms = sum(plain_form_solve_ms(inst.n, int(k), 10, dtype) for inst, k in zip(insts, steps))
+        cost = {n: plain_form_costs(n, dtype) for n in sorted({i.n for i in insts})}
+        ms = sum(int(k) * cost[inst.n][0] + (int(k) // 10) * cost[inst.n][1] for inst, k in zip(insts, steps))
         plain[name] = ms / 1e3
     torch.cuda.empty_cache()
     return {"instances": len(insts), "grids": sorted({i.n for i in insts}),
@@ -603,10 +614,7 @@ def batched_leg():
             "speedup": t_alone / t_batch,
             "plain_form_solves_per_s": {k: len(insts) / v for k, v in plain.items()},
             "speedup_vs_plain_form": {k: v / t_batch for k, v in plain.items()},
-            "plain_form": "the reference's per-step sequence looped from Python (cuFFT via torch.fft, "
-                          "byte-equivalent elementwise kernels, normalise every step, energy check every "
-                          "10 steps), one solve at a time for the steps each solve took; c128 as the "
-                          "reference ships, c64 for comparison; device time (a floor on its wall time)",
+            "plain_form": PLAIN_FORM_NOTE,
             "psi_err_vs_fp64_same_dt": psi_err,
             "steps_median": int(np.median(steps)), "steps_max": int(steps.max()),
             "same_steps_as_alone": bool(np.array_equal(steps, a_steps)),
@@ -619,20 +627,23 @@ def batched_leg():
 SERVE_MAX_ACTIVE = 8
 
 
-def serving_leg(count, rates, plain_sample):
+def serving_leg(count, rates, measure_one_at_a_time=False):
     """Serving stream (config 5): ``count`` requests with seeded Poisson arrivals at
     each rate of ``rates``; 70% imaginary-time ground states 32^3..128^3 and 30%
     real-time stirring segments of 500-5000 steps on 8 resident states
-    64^3..256^3, complex64, 150 GB budget and the device's free memory.  The
-    continuous-batching server against one request at a time through single
-    plans on the same stream (results must be identical), and, on the first
-    ``plain_sample`` requests, against the reference's plain form one request at
-    a time (its per-step sequence for the steps each request took; service time
-    only, no arrival gaps, so an upper bound on its throughput)."""
+    64^3..256^3, complex64, 150 GB budget and the device's free memory, through
+    the continuous-batching server (measured, wall clock).
+
+    One request at a time on the same arrivals: a FIFO schedule over each
+    request's service time alone, for this library's single plans (set-up, steps
+    and checks at per-size costs measured here, times the request's step count)
+    and for the reference's plain form (its per-step sequence, ``plain_form_costs``).
+    With ``measure_one_at_a_time`` the single-plan path also runs the whole stream
+    (``serve.run_plain``) and results are checked identical to the server's."""
     import torch
     from gpe_simulator_b200 import serve
     out = {"requests": count, "max_active_solves": SERVE_MAX_ACTIVE, "budget_bytes": 150e9, "rates": []}
-    first = None
+    grids = [n for n, _ in serve.SESSION_GRIDS]
     for rate in rates:
         reqs = serve.workload(count, rate=rate, seed=2)
         sess = serve.make_sessions()
@@ -641,53 +652,66 @@ def serving_leg(count, rates, plain_sample):
         srv.run(reqs)
         wall = time.perf_counter() - t0
         mixed = serve.summarise(reqs)
-        reqs2 = serve.workload(count, rate=rate, seed=2)
-        sess2 = serve.make_sessions()
-        serve.run_plain(reqs2, sess2)
-        plain = serve.summarise(reqs2)
-        same = all(a.taken == b.taken and (a.kind != "imaginary" or torch.equal(a.result["psi"], b.result["psi"]))
-                   for a, b in zip(reqs, reqs2))
-        same = same and all(torch.equal(x.psi, y.psi) for x, y in zip(sess, sess2))
-        out["rates"].append({
-            "rate_per_s": rate, "imaginary": sum(r.kind == "imaginary" for r in reqs),
-            "solves_per_s": mixed["solves_per_s"], "p50_ms": mixed["p50_ms"], "p99_ms": mixed["p99_ms"],
-            "makespan_s": mixed["makespan_s"], "one_at_a_time_solves_per_s": plain["solves_per_s"],
-            "one_at_a_time_p50_ms": plain["p50_ms"], "one_at_a_time_p99_ms": plain["p99_ms"],
-            "speedup": mixed["solves_per_s"] / plain["solves_per_s"],
-            "admissions_deferred_for_memory": srv.refused,
-            "results_identical_to_one_at_a_time": bool(same), "wall_s": wall})
-        if first is None:
-            first = reqs
-        for s_ in sess + sess2:
-            s_.plan.close()
-        del reqs2
-        torch.cuda.empty_cache()
-    # the reference's plain form on a sample of the stream, one request at a time
-    sample = sorted(first, key=lambda r: r.arrival)[:plain_sample]
-    grids = dict(enumerate(n for n, _ in serve.SESSION_GRIDS))
-    plain_form = {}
-    for name, dtype in (("c128", torch.complex128), ("c64", torch.complex64)):
-        ms = 0.0
-        for r in sample:
+        row = {"rate_per_s": rate, "imaginary": sum(r.kind == "imaginary" for r in reqs),
+               "solves_per_s": mixed["solves_per_s"], "p50_ms": mixed["p50_ms"], "p99_ms": mixed["p99_ms"],
+               "makespan_s": mixed["makespan_s"], "admissions_deferred_for_memory": srv.refused, "wall_s": wall}
+        # one at a time through single plans: FIFO over measured per-size costs
+        sess_model = serve.make_sessions(relax_steps=20)
+        icost, rcost = serve.plan_service_costs(reqs, sess_model)
+
+        def own(r):
             if r.kind == "imaginary":
-                ms += plain_form_solve_ms(r.inst.n, r.taken, 20, dtype)
-            else:
-                ms += plain_form_solve_ms(grids[r.session], r.taken, 0, dtype, real_time=True)
-        plain_form[name] = len(sample) / (ms / 1e3)
-    torch.cuda.empty_cache()
-    top = max(out["rates"], key=lambda d: d["solves_per_s"])
-    out["plain_form_sample_requests"] = len(sample)
-    out["plain_form_solves_per_s"] = plain_form
-    out["speedup_vs_plain_form"] = {k: top["solves_per_s"] / v for k, v in plain_form.items()}
-    out["plain_form"] = ("the reference's per-step sequence (cuFFT via torch.fft, byte-equivalent "
-                         "elementwise kernels, normalise every imaginary step, energy check every 20 "
-                         "steps) one request at a time for the steps each request took, device time "
-                         "without arrival gaps; compared with the server's solves/s at its best rate")
-    # headline keys of the first rate
+                setup, per_chunk = icost[r.inst.n]
+                return setup + (r.taken // 20) * per_chunk
+            per_step, tail = rcost[r.session]
+            return r.taken * per_step + tail
+
+        mod = serve.fifo_summary(reqs, own)
+        row.update({"one_at_a_time_solves_per_s": mod["solves_per_s"], "one_at_a_time_p50_ms": mod["p50_ms"],
+                    "one_at_a_time_p99_ms": mod["p99_ms"], "speedup": mixed["solves_per_s"] / mod["solves_per_s"]})
+        # the reference's plain form, one at a time, on the same arrivals
+        for name, dtype in (("c128", torch.complex128), ("c64", torch.complex64)):
+            icp = {n: plain_form_costs(n, dtype, steps=60, checks=6)
+                   for n in sorted({r.inst.n for r in reqs if r.kind == "imaginary"})}
+            rcp = {n: plain_form_costs(n, dtype, real_time=True, steps=60, checks=2) for n in sorted(set(grids))}
+
+            def plain(r):
+                if r.kind == "imaginary":
+                    step, chk = icp[r.inst.n]
+                    return (r.taken * step + (r.taken // 20) * chk) / 1e3
+                step, chk = rcp[grids[r.session]]
+                return (r.taken * step + chk) / 1e3
+
+            pf = serve.fifo_summary(reqs, plain)
+            row[f"plain_form_{name}"] = {"solves_per_s": pf["solves_per_s"], "p50_ms": pf["p50_ms"],
+                                         "p99_ms": pf["p99_ms"]}
+            row[f"speedup_vs_plain_form_{name}"] = mixed["solves_per_s"] / pf["solves_per_s"]
+        torch.cuda.empty_cache()
+        if measure_one_at_a_time:
+            reqs2 = serve.workload(count, rate=rate, seed=2)
+            sess2 = serve.make_sessions()
+            serve.run_plain(reqs2, sess2)
+            meas = serve.summarise(reqs2)
+            same = all(a.taken == b.taken and (a.kind != "imaginary" or torch.equal(a.result["psi"], b.result["psi"]))
+                       for a, b in zip(reqs, reqs2))
+            same = same and all(torch.equal(x.psi, y.psi) for x, y in zip(sess, sess2))
+            row["one_at_a_time_measured"] = {"solves_per_s": meas["solves_per_s"], "p50_ms": meas["p50_ms"],
+                                             "p99_ms": meas["p99_ms"], "results_identical": bool(same)}
+            for s_ in sess2:
+                s_.plan.close()
+        for s_ in sess + sess_model:
+            s_.plan.close()
+        out["rates"].append(row)
+        torch.cuda.empty_cache()
+    out["one_at_a_time"] = ("FIFO schedule on the same arrivals over each request's time alone: this "
+                            "library's single plans at per-size costs measured here (plan set-up, 20-step "
+                            "chunks with their energy check, per-step cost of each resident session) times "
+                            "the request's steps")
+    out["plain_form"] = PLAIN_FORM_NOTE
     out.update({k: out["rates"][0][k] for k in ("rate_per_s", "solves_per_s", "p50_ms", "p99_ms",
                                                  "one_at_a_time_solves_per_s", "one_at_a_time_p50_ms",
                                                  "one_at_a_time_p99_ms", "speedup",
-                                                 "results_identical_to_one_at_a_time")})
+                                                 "speedup_vs_plain_form_c128", "speedup_vs_plain_form_c64")})
     return out
 
 
@@ -754,8 +778,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=1000, help="requests of the serving stream")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[50.0],
                     help="Poisson arrival rates (requests/s) of the serving stream")
-    ap.add_argument("--serve-plain-sample", type=int, default=100,
-                    help="requests of the stream also run in the reference's plain form")
+    ap.add_argument("--serve-measure-one-at-a-time", action="store_true",
+                    help="also run the whole stream one request at a time through single plans")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -1650,6 +1650,7 @@ struct gpe_batch {
     Sweep* d_sw = nullptr;      // [roles][members]
     int cap = 0;
     cudaStream_t stream = nullptr;
+    int priority = 0;           // of `stream`: that of the stream the batch was last bound on
     cudaEvent_t ev = nullptr;
     int uploaded = 0;           // member count the device arrays hold
     // real time: half-step time and beam centres of every step of the current call,
@@ -2034,9 +2035,15 @@ int gpe_batch_remove(gpe_batch* b, int index) {
     return fail(GPE_ERR_ARG, "no such batch instance");
   // The caller has synchronised the batch's stream (the graph is idle).  Freeing
   // device memory would wait for every stream of the device, so removed plans are
-  // parked and freed together once enough have accumulated.
-  for (auto& g : b->groups) CU(cudaStreamSynchronize(g.stream));
-  batch_free_graph(b);
+  // parked and freed together once enough have accumulated.  An instance that is
+  // not bound (a rebind left it out) leaves without rebuilding the device tables.
+  bool bound = false;
+  for (auto& g : b->groups)
+    bound = bound || std::find(g.members.begin(), g.members.end(), index) != g.members.end();
+  if (bound) {
+    for (auto& g : b->groups) CU(cudaStreamSynchronize(g.stream));
+    batch_free_graph(b);
+  }
   b->psis[index] = nullptr;
   for (auto& g : b->groups) {
     g.all.erase(std::remove(g.all.begin(), g.all.end(), index), g.all.end());
@@ -2044,7 +2051,7 @@ int gpe_batch_remove(gpe_batch* b, int index) {
     g.members.erase(std::remove(g.members.begin(), g.members.end(), index), g.members.end());
     if (g.members.size() != before) TRY(group_upload(b, g));
   }
-  TRY(jobs_upload(b));
+  if (bound) TRY(jobs_upload(b));
   b->parked.push_back(b->plans[index]);
   if (b->parked.size() >= 64) {
     for (auto* q : b->parked) free_plan(q);
@@ -2068,6 +2075,16 @@ int gpe_batch_bind(gpe_batch* b, void* const* psis, const int* active, void* str
   CU(cudaStreamSynchronize((cudaStream_t)stream));
   for (auto& g : b->groups) CU(cudaStreamSynchronize(g.stream));
   batch_free_graph(b);
+  // the groups' streams run at the priority of the caller's stream (a server can put
+  // its batch ahead of long real-time segments on lower-priority streams)
+  int priority = 0;
+  CU(cudaStreamGetPriority((cudaStream_t)stream, &priority));
+  for (auto& g : b->groups)
+    if (g.priority != priority) {
+      CU(cudaStreamDestroy(g.stream));
+      CU(cudaStreamCreateWithPriority(&g.stream, cudaStreamNonBlocking, priority));
+      g.priority = priority;
+    }
   for (int i = 0; i < count; ++i) b->psis[i] = b->plans[i] ? psis[i] : nullptr;
   for (auto& g : b->groups) {
     g.members.clear();

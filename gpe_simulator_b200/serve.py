@@ -119,7 +119,7 @@ class Server:
     real-time segments on per-session streams (see the module docstring)."""
 
     def __init__(self, sessions, dtype=torch.complex64, budget=150e9, chunk=20, max_active=None,
-                 mem_info=None, reserve=2 << 30):
+                 mem_info=None, reserve=2 << 30, batch_priority=True):
         self.sessions = sessions
         self.dtype = dtype
         self.budget = budget
@@ -132,8 +132,12 @@ class Server:
         # at most this many imaginary-time solves advance together (None: as many as
         # the memory budget admits); fewer finish sooner, more share each launch
         self.max_active = max_active
+        # the imaginary-time batch advances in short chunks with a host check after
+        # each, so it runs ahead of the long real-time segments: on the device's
+        # highest stream priority (the batch's own streams follow it), segments at
+        # the default priority
         self.streams = [torch.cuda.Stream() for _ in sessions]
-        self.batch_stream = torch.cuda.Stream()
+        self.batch_stream = torch.cuda.Stream(priority=-100 if batch_priority else 0)
 
     def run(self, requests):
         """Serve ``requests`` against the wall clock (arrival times are offsets from the
@@ -141,6 +145,7 @@ class Server:
         pending = sorted(requests, key=lambda r: r.arrival)
         queue = []
         imag = {}          # batch index -> [request, psi, last E, steps]
+        retired = []       # batch indices of solves finished this round
         real = {}          # session -> (request, completion event)
         used = 0.0
         batch = Batch([], self.dtype)
@@ -216,10 +221,23 @@ class Server:
                     if conv or rec[3] >= r.max_steps:
                         r.done_at, r.taken = now, rec[3]
                         r.result = dict(N=diag[idx, 0], E=e, mu=diag[idx, 5], psi=rec[1])
-                        with torch.cuda.stream(self.batch_stream):
-                            batch.remove(idx)
                         used -= state_bytes(r.inst.n, self.dtype)
                         del imag[idx]
+                        retired.append(idx)
+                if retired:
+                    # one rebind for every retirement of the round (the batch's device
+                    # tables are rebuilt once); the retired instances, no longer bound,
+                    # then leave the batch without another rebuild
+                    with torch.cuda.stream(self.batch_stream):
+                        psis = [None] * len(batch.instances)
+                        act = np.zeros(len(batch.instances), np.int32)
+                        for idx, rec in imag.items():
+                            psis[idx] = rec[1]
+                            act[idx] = 1
+                        batch.bind(psis, act)
+                        for idx in retired:
+                            batch.remove(idx)
+                    retired.clear()
             elif real or queue:
                 time.sleep(2e-4)
             elif pending:
@@ -272,6 +290,64 @@ def run_plain(requests, sessions, dtype=torch.complex64, chunk=20):
         torch.cuda.synchronize()
         r.done_at = time.perf_counter() - t0
     return requests
+
+
+def fifo_summary(requests, service_s):
+    """Latencies and throughput of serving ``requests`` one at a time in arrival
+    order when request ``r`` takes ``service_s(r)`` seconds alone (a request
+    starts when it has arrived and the previous one is done)."""
+    done, lat, first = 0.0, [], None
+    for r in sorted(requests, key=lambda q: q.arrival):
+        first = r.arrival if first is None else first
+        done = max(done, r.arrival) + service_s(r)
+        lat.append(done - r.arrival)
+    lat = np.array(lat)
+    span = done - first
+    return dict(requests=len(lat), solves_per_s=len(lat) / span, makespan_s=span,
+                p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3))
+
+
+def plan_service_costs(requests, sessions, dtype=torch.complex64, chunk=20, reps=5):
+    """Seconds that ``run_plain`` spends on one request of each kind and size, by
+    parts: an imaginary-time solve's set-up (plan, initial state, release) and
+    each ``chunk`` steps with their energy check; a real-time segment's seconds
+    per step (one multi-step call) and its closing norm.  Measured on this GPU."""
+    imag = {}
+    for n in sorted({r.inst.n for r in requests if r.kind == "imaginary"}):
+        inst = next(r.inst for r in requests if r.kind == "imaginary" and r.inst.n == n)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            plan = Plan(inst.n, inst.x, inst.k, dtype=dtype, kind="imaginary", beta=inst.beta, dt=inst.dt,
+                        static_expr=inst.static_expr)
+            psi = initial_states([inst], dtype, seed0=1)[0]
+            plan.close()
+        torch.cuda.synchronize()
+        setup = (time.perf_counter() - t0) / reps
+        plan = Plan(inst.n, inst.x, inst.k, dtype=dtype, kind="imaginary", beta=inst.beta, dt=inst.dt,
+                    static_expr=inst.static_expr)
+        plan.step(psi, chunk)
+        plan.diagnostics(psi)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            plan.step(psi, chunk)
+            plan.diagnostics(psi)
+        per_chunk = (time.perf_counter() - t0) / reps
+        plan.close()
+        imag[n] = (setup, per_chunk)
+    real = {}
+    for s_, sess in enumerate(sessions):
+        psi = sess.psi.clone()
+        sess.plan.step(psi, 10, 0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sess.plan.step(psi, 200, 10)
+        torch.cuda.synchronize()
+        per_step = (time.perf_counter() - t0) / 200
+        t0 = time.perf_counter()
+        sess.plan.norm(psi)
+        real[s_] = (per_step, time.perf_counter() - t0)
+    return imag, real
 
 
 def summarise(requests):
