@@ -1,7 +1,7 @@
 """Run the reference's own propagator code on the host CPU.
 
 TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).  Works only where the
-reference sources are present (``GPE_REFERENCE`` or ``/root/reference``); it is
+reference sources are present and ``GPE_REFERENCE`` names their root; it is
 used to generate the golden fixtures in ``tests/golden`` and to pin the
 ``oracle.ssf`` restatement against the reference itself.
 
@@ -37,15 +37,15 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-# This recipe reads the reference's sources where the build container mounts
-# them; GPE_REFERENCE points it elsewhere.  Nothing on the product path, in the
-# GPU tests or in the bench reads them.
-REFERENCE = Path(os.environ.get("GPE_REFERENCE", "/root/reference"))
+# The reference's source tree, from GPE_REFERENCE (no default): nothing on the
+# product path, in the GPU tests or in the bench reads it.
+REFERENCE = Path(os.environ["GPE_REFERENCE"]) if os.environ.get("GPE_REFERENCE") else None
+UNSET = "GPE_REFERENCE is unset: set it to the reference's source tree to run the reference on the host"
 
 
 def available():
-    """True when the reference's sources are present for this recipe."""
-    return (REFERENCE / "gpe" / "make_propagator.py").exists()
+    """True when GPE_REFERENCE names a tree holding the reference's sources."""
+    return REFERENCE is not None and (REFERENCE / "gpe" / "make_propagator.py").exists()
 
 _COMPLEX_HEADER = r"""
 #pragma once
@@ -323,7 +323,9 @@ class HostReductionKernel:
 
 def install():
     """Install the shim as ``cupy`` and import the reference package ``gpe``."""
-    if not (REFERENCE / "gpe" / "make_propagator.py").exists():
+    if REFERENCE is None:
+        raise RuntimeError(UNSET)
+    if not available():
         raise RuntimeError(f"reference sources not found at {REFERENCE}")
     cupy = ModuleType("cupy")
     cupy.__getattr__ = lambda name: getattr(np, name)

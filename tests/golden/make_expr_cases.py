@@ -42,7 +42,7 @@ CORPUS = [
 def main():
     from oracle import ref_shim
     if not ref_shim.available():
-        raise SystemExit("the reference sources are not present")
+        raise SystemExit(ref_shim.UNSET if ref_shim.REFERENCE is None else "the reference sources are not present")
     sys.path.insert(0, str(ref_shim.REFERENCE))
     from gpe.expressions import cuda_expression   # pure Python in the reference
     rows = []

@@ -1,7 +1,7 @@
 """Generate the golden fixtures from the reference implementation itself.
 
-Runs ONLY where the reference sources are present (``GPE_REFERENCE`` or
-``/root/reference``).  The reference's own ``gpe`` package is imported with a
+Runs ONLY where ``GPE_REFERENCE`` names the reference's source tree.  The
+reference's own ``gpe`` package is imported with a
 NumPy-backed CuPy (``oracle/ref_shim.py``): its propagator closures
 (``gpe/make_propagator.py``), its CUDA kernel strings compiled for the host
 (``gpe/kernels.py``, ``gpe/make_kernel.py``, ``gpe/helper.py``) and its

@@ -1,6 +1,11 @@
 """Snapshots in the reference's format (``gpe/state_io.py``): round trips across
-precisions, the reference's checks, and files exchanged with the reference's own
-save/load (run on the host through the oracle shim, where the reference exists)."""
+precisions, the reference's checks, the files the reference's own
+``save_wavefunction`` wrote (``tests/golden/state_ref``, made by
+``tests/golden/make_state_files.py``), and a live exchange with the reference's
+save/load run on the host through the oracle shim where GPE_REFERENCE is set."""
+
+import json
+from pathlib import Path
 
 from types import SimpleNamespace
 
@@ -10,7 +15,9 @@ import torch
 
 from gpe_simulator_b200.state_io import load_wavefunction, save_wavefunction
 
-from oracle.ref_shim import REFERENCE  # noqa: E402
+from oracle import ref_shim  # noqa: E402
+
+STATE_REF = Path(__file__).resolve().parent / "golden" / "state_ref"
 
 
 def make_stage(n=8, L=6.0, dtype=torch.complex64, seed=0):
@@ -53,9 +60,26 @@ def test_load_rejects_what_the_reference_rejects(tmp_path):
         load_wavefunction(tmp_path / "b.npy", st)
 
 
-@pytest.mark.skipif(not REFERENCE.exists(), reason="the reference is not present")
+def test_files_written_by_the_reference_load_and_match_ours_byte_for_byte(tmp_path):
+    """The reference's snapshot of the seeded stage loads in both precisions; our
+    save of the same stage gives the same .npy bytes, metadata and axes."""
+    st = make_stage(dtype=torch.complex128)
+    for dtype in (torch.complex128, torch.complex64):
+        back = load_wavefunction(STATE_REF / "psi_00000004.npy", st, dtype)
+        assert back.dtype == dtype and torch.equal(back, st.psi.to(dtype))
+    save_wavefunction(tmp_path / "psi_00000004.npy", st, 4)
+    assert (tmp_path / "psi_00000004.npy").read_bytes() == (STATE_REF / "psi_00000004.npy").read_bytes()
+    assert (json.loads((tmp_path / "psi_00000004.json").read_text())
+            == json.loads((STATE_REF / "psi_00000004.json").read_text()))
+    with np.load(tmp_path / "grid.npz") as ours, np.load(STATE_REF / "grid.npz") as theirs:
+        assert sorted(ours.files) == sorted(theirs.files) == ["k_array", "x_array"]
+        for name in ours.files:
+            np.testing.assert_array_equal(ours[name], theirs[name])
+
+
+@pytest.mark.skipif(not ref_shim.available(), reason=ref_shim.UNSET if ref_shim.REFERENCE is None
+                    else "no reference sources where GPE_REFERENCE points")
 def test_files_exchange_with_the_reference(tmp_path):
-    from oracle import ref_shim
     ref = ref_shim.install()
     st = make_stage(dtype=torch.complex128)
     save_wavefunction(tmp_path / "ours" / "psi.npy", st, 3)
