@@ -19,6 +19,8 @@
 // lanes walk across lines, 128-byte rows).  Pointwise work (renormalisation,
 // half-steps, 1/M, kinetic phase, norm partials) runs on the registers.
 #pragma once
+#include <type_traits>
+
 #include "gpe_kernels.cuh"
 
 namespace gpe {
@@ -32,7 +34,9 @@ template <> struct Split<96>  { static constexpr int N1 = 12, N2 = 8;  };
 template <> struct Split<128> { static constexpr int N1 = 8,  N2 = 16; };
 template <> struct Split<160> { static constexpr int N1 = 10, N2 = 16; };
 template <> struct Split<256> { static constexpr int N1 = 16, N2 = 16; };
-template <> struct Split<512> { static constexpr int N1 = 32, N2 = 16; };
+// n = 512: three radix-8 phases over 64 lanes (fft_3phase); N1 = 64 lanes and
+// N2 = 8 values per slot in every layout
+template <> struct Split<512> { static constexpr int N1 = 64, N2 = 8; };
 
 __host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
 
@@ -56,13 +60,16 @@ __host__ __device__ constexpr int fast_lines(int n, int real_bytes) {
 template <int N, typename R> struct FastCfg {
   static constexpr int L = fast_lines(N, (int)sizeof(R));
   static constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
-  static constexpr int P1 = L * N1, P2 = L * N2;
-  static constexpr bool POW2 = (N & (N - 1)) == 0 && N <= 256;
+  // three-phase transform (n = 512): the layout (N1 lanes, N2 values) in and out
+  static constexpr bool THREE = N == 512;
+  static constexpr int P1 = L * N1, P2 = THREE ? P1 : L * N2;
+  static constexpr bool POW2 = (N & (N - 1)) == 0 && N <= 512;
   // power-of-two sizes: 16 values per thread; other sizes: one slot per thread per phase
   static constexpr int T0 = POW2 ? L * N / 16 : cdiv(P1 > P2 ? P1 : P2, 32) * 32;
   static constexpr int T = T0 < 32 ? 32 : T0;
   static constexpr int Q1 = cdiv(P1, T), Q2 = cdiv(P2, T);
-  static constexpr int V = Q1 * N2 > Q2 * N1 ? Q1 * N2 : Q2 * N1;   // registers (complex) per thread
+  // registers (complex) per thread
+  static constexpr int V = THREE ? Q1 * N2 : (Q1 * N2 > Q2 * N1 ? Q1 * N2 : Q2 * N1);
 };
 
 enum : int { FZ = 0, FY = 1, FX = 2 };
@@ -119,7 +126,8 @@ template <int N, typename R> __host__ __device__ constexpr size_t fast_smem_byte
                * sizeof(typename Cx<R>::T)
          + 32 * 4 * 16                                          /* Acc reduction */
          + fast_tables_bytes<N, R>()
-         + (Split<N>::N1 == Split<N>::N2 ? 0 : (size_t)(2 * N) * sizeof(typename Cx<R>::T));  /* t2 */
+         + (FastCfg<N, R>::THREE ? (size_t)64 * sizeof(typename TwE<R>::T)          /* t2: W_64 */
+            : Split<N>::N1 == Split<N>::N2 ? 0 : (size_t)(2 * N) * sizeof(typename Cx<R>::T));  /* t2 */
 }
 
 template <int N, int AX, typename R>
@@ -150,12 +158,18 @@ struct FastTile {
   __device__ __forceinline__ long long gidx(int l, int m) const { return base + l * lstride + (long long)m * nstride; }
 };
 
-// Slot s of thread t in a phase with `per` lanes per line: Z tiles walk along the
-// line (lane fastest), P tiles across lines (line fastest).
-template <int AX, int LL>
+// Slot s of thread t (gs = t + s*TT) in a phase with `per` lanes per line: Z tiles
+// walk along the line (lane fastest), P tiles across lines (line fastest).  Z
+// tiles of one warp per line (TT = 32 LL) with more than 32 lanes give each
+// thread lanes t%32 + 32 s of line t/32, so that a line stays in its warp.
+template <int AX, int LL, int TT>
 __device__ __forceinline__ void slot(int gs, int per, int& l, int& lane) {
-  if (AX == FZ) { lane = gs % per; l = gs / per; }
-  else { l = gs % LL; lane = gs / LL; }
+  if (AX == FZ) {
+    if (TT == 32 * LL && per > 32) { const int t = gs % TT; l = t >> 5; lane = (t & 31) + 32 * (gs / TT); }
+    else { lane = gs % per; l = gs / per; }
+  } else {
+    l = gs % LL; lane = gs / LL;
+  }
 }
 
 // One forward FFT of every line of the tile, A = lanes in phase 1 (values A-strided),
@@ -183,7 +197,7 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
     const int gs = threadIdx.x + s * T;
     if (QA * T > L * A && gs >= L * A) break;
     int l, lane;
-    slot<AX, L>(gs, A, l, lane);
+    slot<AX, L, T>(gs, A, l, lane);
     C* x = v + s * B;
     Dft<B>::run(x, (const C*)nullptr, (const C*)nullptr, N / B);
 #pragma unroll
@@ -202,7 +216,7 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
     const int gs = threadIdx.x + s * T;
     if (QB * T > L * B && gs >= L * B) break;
     int l, k2;
-    slot<AX, L>(gs, B, l, k2);
+    slot<AX, L, T>(gs, B, l, k2);
     C* x = v + s * A;
 #pragma unroll
     for (int n1 = 0; n1 < A; ++n1) {
@@ -213,6 +227,80 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
   }
   if (ASYNC_NEXT) fence_proxy_async_smem();
   if (WARP_LOCAL) __syncwarp(); else __syncthreads();
+}
+
+// One forward FFT of every line of the tile for N = 8^3 (n = 512), in three
+// radix-8 phases over 64 lanes per line.  In and out the registers are in
+// layout (64 lanes, 8 values): slot s of lane p holds v[s][b] = x[p + 64 b] on
+// entry and X[p + 64 k] on return, so the two transforms of a fused sweep need
+// no change of layout between them.  Index split: n = p + 64 b with p = p1 + 8 p2,
+// k = k3 + 8 k1 + 64 k2.
+//   phase 1 (lane p):         DFT8 over b -> k3, times W_512^(p k3)     (twa[k3*64 + p])
+//   phase 2 (role p1 + 8 k3): DFT8 over p2 -> k1, times W_64^(p1 k1)    (twb[k1*8 + p1])
+//   phase 3 (role k3 + 8 k1): DFT8 over p1 -> k2; lane k3 + 8 k1 holds X[lane + 64 k2]
+// Exchange layouts: Z tiles (a warp per line) rows of 72 elements per (line, k),
+// the second exchange with a pitch of 9 per p1, so that 8-byte accesses of a
+// half warp avoid bank conflicts; P tiles line-fastest, [k][role][l].
+template <int N, int AX, typename R, int Q, int V>
+__device__ __forceinline__ void fft_3phase(typename Cx<R>::T (&v)[V], typename Cx<R>::T* ex,
+                                           const typename TwE<R>::T* twa, const typename TwE<R>::T* twb) {
+  using C = typename Cx<R>::T;
+  constexpr int L = FastCfg<N, R>::L;
+  constexpr int T = FastCfg<N, R>::T;
+  constexpr int RD = 8, A = 64;
+  static_assert(N == RD * RD * RD && Q * RD <= V && Q * T == L * A, "three-phase layout");
+  constexpr bool WARP_LOCAL = AX == FZ && T == 32 * L;
+  auto e1 = [](int l, int k3, int p) { return AX == FZ ? (l * RD + k3) * 72 + p : (k3 * A + p) * L + l; };
+  auto e2 = [](int l, int k3, int k1, int p1) {
+    return AX == FZ ? (l * RD + k1) * 72 + 9 * p1 + k3 : ((k1 * RD + k3) * RD + p1) * L + l;
+  };
+  auto sync = [] { if (WARP_LOCAL) __syncwarp(); else __syncthreads(); };
+#pragma unroll
+  for (int s = 0; s < Q; ++s) {
+    int l, p;
+    slot<AX, L, T>(threadIdx.x + s * T, A, l, p);
+    C* x = v + s * RD;
+    Dft<RD>::run(x, (const C*)nullptr, (const C*)nullptr, N / RD);
+#pragma unroll
+    for (int k3 = 1; k3 < RD; ++k3) x[k3] = tw_apply(x[k3], twa[k3 * A + p]);
+#pragma unroll
+    for (int k3 = 0; k3 < RD; ++k3) ex[e1(l, k3, p)] = x[k3];
+  }
+  sync();
+#pragma unroll
+  for (int s = 0; s < Q; ++s) {
+    int l, q;
+    slot<AX, L, T>(threadIdx.x + s * T, A, l, q);
+    const int p1 = q & 7, k3 = q >> 3;
+    C* x = v + s * RD;
+#pragma unroll
+    for (int p2 = 0; p2 < RD; ++p2) x[p2] = ex[e1(l, k3, p1 + RD * p2)];
+  }
+  sync();
+#pragma unroll
+  for (int s = 0; s < Q; ++s) {
+    int l, q;
+    slot<AX, L, T>(threadIdx.x + s * T, A, l, q);
+    const int p1 = q & 7, k3 = q >> 3;
+    C* x = v + s * RD;
+    Dft<RD>::run(x, (const C*)nullptr, (const C*)nullptr, N / RD);
+#pragma unroll
+    for (int k1 = 1; k1 < RD; ++k1) x[k1] = tw_apply(x[k1], twb[k1 * RD + p1]);
+#pragma unroll
+    for (int k1 = 0; k1 < RD; ++k1) ex[e2(l, k3, k1, p1)] = x[k1];
+  }
+  sync();
+#pragma unroll
+  for (int s = 0; s < Q; ++s) {
+    int l, q;
+    slot<AX, L, T>(threadIdx.x + s * T, A, l, q);
+    const int k3 = q & 7, k1 = q >> 3;
+    C* x = v + s * RD;
+#pragma unroll
+    for (int p1 = 0; p1 < RD; ++p1) x[p1] = ex[e2(l, k3, k1, p1)];
+    Dft<RD>::run(x, (const C*)nullptr, (const C*)nullptr, N / RD);
+  }
+  sync();
 }
 
 template <typename R>
@@ -282,12 +370,17 @@ struct FastTables {
   double* kyz2;   // [L] k_j^2 + k_kl^2
 };
 
+// two: the tables of the fused z sweep (c2, c12 at the second half-step's time).
+// pre (real time, two half-steps as one rotation, no potential arrays): vz and
+// c12 are stored already multiplied by dt (vz by dt, c12 by dt/2), so that the
+// phase (2 vz + c12 + 2 beta |psi|^2) dt/2 is one add and one fma per point.
 template <int N, typename R>
 __device__ __forceinline__ void z_tables(const Phys& ph, const Sweep& sw, int a0, FastTables<R>& tb,
-                                         bool two) {
+                                         bool two, bool pre = false) {
   constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
   const R* vax = (const R*)ph.vax;
-  for (int q = threadIdx.x; q < N; q += T) tb.vz[q] = vax[2 * N + q];
+  const R h = (R)(ph.dt * 0.5), dt2 = h + h;
+  for (int q = threadIdx.x; q < N; q += T) tb.vz[q] = pre ? vax[2 * N + q] * dt2 : vax[2 * N + q];
   if (threadIdx.x < L) {
     const int g = a0 + threadIdx.x, i = g / N, j = g % N;
     const R base = vax[i] + vax[N + j];
@@ -309,7 +402,7 @@ __device__ __forceinline__ void z_tables(const Phys& ph, const Sweep& sw, int a0
     }
     tb.c1[threadIdx.x] = base + b1;
     tb.c2[threadIdx.x] = base + b2;
-    tb.c12[threadIdx.x] = (base + b1) + (base + b2);
+    tb.c12[threadIdx.x] = pre ? ((base + b1) + (base + b2)) * h : (base + b1) + (base + b2);
   }
 }
 
@@ -367,7 +460,7 @@ __device__ __forceinline__ void kin_all(typename Cx<R>::T (&v)[EPT], const Phys&
   for (int s = 0; s < SLOTS; ++s) {
     if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
     int l, lane;
-    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+    slot<AX, L, T>(threadIdx.x + s * T, LANES, l, lane);
 #pragma unroll
     for (int a = 0; a < VALS; ++a) v[s * VALS + a] = fast_kin<R, REAL, CUT>(ph, tb, v[s * VALS + a], lane + LANES * a, l);
   }
@@ -383,7 +476,8 @@ __device__ __forceinline__ void kin_all(typename Cx<R>::T (&v)[EPT], const Phys&
 // keeps the fused sweeps within their register budget.
 // TWO: two consecutive real-time half-steps at one point as one rotation by
 // (2 vz[m] + ctab[l] + 2 beta |psi|^2) dt/2 with ctab = c1 + c2; exact because
-// the first rotation leaves |psi| unchanged (callers pass beta already doubled).
+// the first rotation leaves |psi| unchanged.  The tables come prescaled (vz[m]
+// by dt, ctab by dt/2, see z_tables) and callers pass beta as 2 beta dt/2.
 template <int N, int AX, typename R, int LANES, int VALS, int SLOTS, int EPT, bool REAL, bool ARR,
           bool TWO = false>
 __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const FastTile<N, AX, R>& tl,
@@ -391,25 +485,27 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
                                          R beta, R h) {
   constexpr int L = FastCfg<N, R>::L, T = FastCfg<N, R>::T;
   static_assert(SLOTS * VALS <= 64, "pending mask");
-  unsigned long long pend = 0ull;   // complex64: elements whose phase exceeds the short series' range
+  // complex64: elements whose phase exceeds the short series' range
+  using Mask = typename std::conditional<(SLOTS * VALS <= 32), unsigned, unsigned long long>::type;
+  Mask pend = 0;
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) {
     if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
     int l, lane;
-    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+    slot<AX, L, T>(threadIdx.x + s * T, LANES, l, lane);
     const long long row = tl.base + (long long)l * tl.lstride;
     const R c = ctab[l];
 #pragma unroll
     for (int a = 0; a < VALS; ++a) {
       const int e = s * VALS + a, m = lane + LANES * a;
-      R V = TWO ? (R)2 * tb.vz[m] + c : tb.vz[m] + c;
+      R V = tb.vz[m] + c;
       R g = (R)0;
       if (ARR) {
         V += ph.vre ? ((const R*)ph.vre)[row + m] : (R)0;
         g = ph.vim ? ((const R*)ph.vim)[row + m] * h : (R)0;
       }
       const typename Cx<R>::T x = v[e];
-      const R phs = (V + beta * (x.x * x.x + x.y * x.y)) * h;
+      const R phs = TWO ? fma(beta, x.x * x.x + x.y * x.y, V) : (V + beta * (x.x * x.x + x.y * x.y)) * h;
       if (sizeof(R) == 8) {
         if (!REAL) {
           const double f = exp(-(double)phs);
@@ -431,32 +527,32 @@ __device__ __forceinline__ void half_all(typename Cx<R>::T (&v)[EPT], const Fast
           v[e] = mk(fma(x.x, (R)cm1, fma(x.y, (R)sn, x.x)), fma(x.y, (R)cm1, fma(-x.x, (R)sn, x.y)));
         }
       } else {
-        pend |= 1ull << e;
+        pend |= (Mask)1 << e;
       }
     }
   }
-  if (sizeof(R) == 8 || !__any_sync(0xffffffffu, pend != 0ull)) return;
+  if (sizeof(R) == 8 || !__any_sync(0xffffffffu, pend != 0)) return;
   // second pass over the elements left unrotated: full series up to pi/4 (1/2 in
   // imaginary time), library functions beyond
 #pragma unroll
   for (int s = 0; s < SLOTS; ++s) {
     if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
     int l, lane;
-    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+    slot<AX, L, T>(threadIdx.x + s * T, LANES, l, lane);
     const long long row = tl.base + (long long)l * tl.lstride;
     const R c = ctab[l];
 #pragma unroll
     for (int a = 0; a < VALS; ++a) {
       const int e = s * VALS + a, m = lane + LANES * a;
-      if (!((pend >> e) & 1ull)) continue;
-      R V = TWO ? (R)2 * tb.vz[m] + c : tb.vz[m] + c;
+      if (!((pend >> e) & 1)) continue;
+      R V = tb.vz[m] + c;
       R g = (R)0;
       if (ARR) {
         V += ph.vre ? ((const R*)ph.vre)[row + m] : (R)0;
         g = ph.vim ? ((const R*)ph.vim)[row + m] * h : (R)0;
       }
       const typename Cx<R>::T x = v[e];
-      const float p = (float)((V + beta * (x.x * x.x + x.y * x.y)) * h);
+      const float p = (float)(TWO ? fma(beta, x.x * x.x + x.y * x.y, V) : (V + beta * (x.x * x.x + x.y * x.y)) * h);
       if (!REAL) {
         const float em = fabsf(p) <= 0.5f ? expm1_series(-p) : expm1f(-p);
         v[e] = mk(fma(x.x, (R)em, x.x), fma(x.y, (R)em, x.y));
@@ -503,7 +599,7 @@ __device__ __forceinline__ void diag_real_all(const typename Cx<R>::T (&v)[EPT],
   for (int s = 0; s < SLOTS; ++s) {
     if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
     int l, lane;
-    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+    slot<AX, L, T>(threadIdx.x + s * T, LANES, l, lane);
     double n0 = 0.0, n1 = 0.0, n2 = 0.0;
 #pragma unroll
     for (int a = 0; a < VALS; ++a) {
@@ -538,7 +634,7 @@ __device__ __forceinline__ void diag_k_all(const typename Cx<R>::T (&v)[EPT], co
   for (int s = 0; s < SLOTS; ++s) {
     if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
     int l, lane;
-    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+    slot<AX, L, T>(threadIdx.x + s * T, LANES, l, lane);
     double e = 0.0;
 #pragma unroll
     for (int a = 0; a < VALS; ++a) {
@@ -588,8 +684,8 @@ __device__ __forceinline__ void fast_pointwise(typename Cx<R>::T (&v)[EPT], cons
   // (1/M was applied with the kinetic factor in the x sweep)
   if (MODE == FM_Z21 && ph.kind == 1 && ph.vre == nullptr && ph.vim == nullptr) {
     // real time, potential from tables: the two half-steps as one rotation
-    half_all<N, AX, R, LANES, VALS, SLOTS, EPT, true, false, true>(v, tl, ph, tb, tb.c12, (R)(2.0 * ph.beta),
-                                                                   (R)(ph.dt * 0.5));
+    const R h = (R)(ph.dt * 0.5);
+    half_all<N, AX, R, LANES, VALS, SLOTS, EPT, true, false, true>(v, tl, ph, tb, tb.c12, (R)(2.0 * ph.beta) * h, h);
     return;
   }
   half_dispatch<N, AX, R, LANES, VALS, SLOTS, EPT>(v, tl, ph, tb, tb.c1);
@@ -622,7 +718,7 @@ __device__ __forceinline__ void fast_load(typename Cx<R>::T (&v)[EPT], const Fas
   for (int s = 0; s < S1; ++s) {
     if (!slot_ok<N, R, N1, S1>(s)) break;
     int l, lane;
-    slot<AX, L>(threadIdx.x + s * T, N1, l, lane);
+    slot<AX, L, T>(threadIdx.x + s * T, N1, l, lane);
 #pragma unroll
     for (int b = 0; b < N2; ++b) {
       const typename Cx<R>::T x = CG ? __ldcg(src + tl.gidx(l, lane + N1 * b)) : src[tl.gidx(l, lane + N1 * b)];
@@ -639,7 +735,7 @@ __device__ __forceinline__ void fast_store(const typename Cx<R>::T (&v)[EPT], co
   for (int s = 0; s < SLOTS; ++s) {
     if (!slot_ok<N, R, LANES, SLOTS>(s)) break;
     int l, lane;
-    slot<AX, L>(threadIdx.x + s * T, LANES, l, lane);
+    slot<AX, L, T>(threadIdx.x + s * T, LANES, l, lane);
 #pragma unroll
     for (int a = 0; a < VALS; ++a) dst[tl.gidx(l, lane + LANES * a)] = v[s * VALS + a];
   }
@@ -684,6 +780,10 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   constexpr int S1 = FastCfg<N, R>::Q1;   // slots in layout (N1 lanes, N2 values)
   constexpr int S2 = FastCfg<N, R>::Q2;   // slots in layout (N2 lanes, N1 values)
   constexpr bool ZM = MODE == FM_Z1 || MODE == FM_Z2 || MODE == FM_Z21;
+  // layout between the transforms: (N2 lanes, N1 values) after a two-phase
+  // transform, (N1, N2) again after the three-phase one
+  constexpr bool THREE = FastCfg<N, R>::THREE;
+  constexpr int LM = THREE ? N1 : N2, VM = THREE ? N2 : N1, SM = THREE ? S1 : S2;
   using TW = typename TwE<R>::T;
   griddep_launch_dependents();
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -715,12 +815,17 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
     for (int q = threadIdx.x; q < N; q += T) {
       const int k2 = q / N1, n1 = q % N1;   // t1[k2*N1 + n1] = W^(n1*k2), n1*k2 < N
       t1[q] = entry(n1 * k2);
-      if (N1 != N2) {
+      if (THREE) {
+        // second-phase table of the three-phase transform: t2[k1*8 + p1] = W_64^(p1*k1)
+        if (q < 64) t2[q] = entry(8 * ((q % 8) * (q / 8)));
+      } else if (N1 != N2) {
         const int k2b = q / N2, n2 = q % N2;  // t2[k1*N2 + n2] = W^(n2*k1)
         t2[q] = entry(n2 * k2b);
       }
     }
-    if (ZM || (MODE == FM_DIAGR && ph.ltab)) z_tables<N, R>(ph, sw, tl.a0, tb, MODE == FM_Z21);
+    if (ZM || (MODE == FM_DIAGR && ph.ltab))
+      z_tables<N, R>(ph, sw, tl.a0, tb, MODE == FM_Z21,
+                     MODE == FM_Z21 && ph.kind == 1 && ph.vre == nullptr && ph.vim == nullptr);
     if (MODE == FM_XKIN) x_tables<N, R>(ph, tl.a0, tl.b0, tb);
     // diagnostic x sweep: the shell histogram takes the tables region
     if (MODE == FM_DIAGK && sw.hist)
@@ -759,20 +864,22 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   __syncthreads();  // twiddles and tables visible
   if (MODE == FM_Z1) fast_pointwise<N, AX, R, MODE, 0, N1, N2, S1>(v, tl, ph, tb, op, cx);
   if (MODE == FM_DIAGR) diag_real_all<N, AX, R, N1, N2, S1>(v, tl, ph, tb, cx);
-  fft_2phase<N, N1, N2, AX, R, S1, S2, EPT>(v, ex, t1);
+  if constexpr (THREE) fft_3phase<N, AX, R, S1, EPT>(v, ex, t1, t2);
+  else fft_2phase<N, N1, N2, AX, R, S1, S2, EPT>(v, ex, t1);
   if (MODE == FM_Z21 || MODE == FM_XKIN) {
     if (MODE == FM_Z21) conj_all(v);  // finish the inverse before the physics
-    fast_pointwise<N, AX, R, MODE, 1, N2, N1, S2>(v, tl, ph, tb, op, cx);
+    fast_pointwise<N, AX, R, MODE, 1, LM, VM, SM>(v, tl, ph, tb, op, cx);
     if (MODE == FM_XKIN) conj_all(v);  // start the inverse
-    fft_2phase<N, N2, N1, AX, R, S2, S1, EPT>(v, ex, t2);
+    if constexpr (THREE) fft_3phase<N, AX, R, S1, EPT>(v, ex, t1, t2);
+    else fft_2phase<N, N2, N1, AX, R, S2, S1, EPT>(v, ex, t2);
     if (MODE == FM_XKIN) conj_all(v);
     fast_store<N, AX, R, N1, N2, S1>(v, tl, (C*)sw.dst);
   } else {
     if (MODE == FM_Z2 || (MODE == FM_PLAIN && op.inv1)) conj_all(v);
-    if (MODE == FM_Z2) fast_pointwise<N, AX, R, MODE, 2, N2, N1, S2>(v, tl, ph, tb, op, cx);
+    if (MODE == FM_Z2) fast_pointwise<N, AX, R, MODE, 2, LM, VM, SM>(v, tl, ph, tb, op, cx);
     if (MODE == FM_PLAIN && op.invm) scale_all(v, (R)ph.inv_m);
-    if (MODE == FM_DIAGK) diag_k_all<N, AX, R, N2, N1, S2>(v, tl, ph, cx);
-    else fast_store<N, AX, R, N2, N1, S2>(v, tl, (C*)sw.dst);
+    if (MODE == FM_DIAGK) diag_k_all<N, AX, R, LM, VM, SM>(v, tl, ph, cx);
+    else fast_store<N, AX, R, LM, VM, SM>(v, tl, (C*)sw.dst);
   }
   if (MODE == FM_Z2 && op.norm) {
     Acc a[1] = {cx.acc[0]};
@@ -799,10 +906,10 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
 // except Z21 and XKIN at n = 256, which run 4 blocks of 64 registers (a few
 // hundred bytes of spills in Z21): 4486 -> 4541 steps/s at 256^3, the gain
 // being in the overlap of the programmatically launched sweeps.
-// At n = 512 (32-point phase, up to 214 registers unbounded; 512-thread
-// blocks) one block per SM: plain sweeps 95 registers, fused ones 128 with a
-// few hundred bytes of spills in Z21/Z2 (bounds measured 240 -> 291 steps/s at
-// 512^3 with 8-line tiles).
+// At n = 512 (three radix-8 phases, 16 values per thread, 512-thread blocks of
+// about 98 KB of shared memory) two blocks per SM, 64 registers: 378 -> 415
+// steps/s at 512^3 against the earlier 32 x 16 split (32 values per thread, one
+// block of 128 registers per SM).
 // The diagnostic z sweep (FP64 potential per point) keeps 512 threads per SM.
 template <int N, typename R, int MODE> struct FastBounds {
   static constexpr int value = (sizeof(R) == 4 && (N == 128 || N == 256))
@@ -810,7 +917,7 @@ template <int N, typename R, int MODE> struct FastBounds {
                                       : (N == 256 && (MODE == FM_Z21 || MODE == FM_XKIN)) ? 1024 : 768) /
                                          FastCfg<N, R>::T
                                : (sizeof(R) == 4 && N == 512)
-                                   ? (MODE == FM_PLAIN ? 768 : 512) / FastCfg<N, R>::T : 0;
+                                   ? (MODE == FM_DIAGR ? 512 : 1024) / FastCfg<N, R>::T : 0;
 };
 
 template <int N, int AX, typename R, int MODE>

@@ -190,7 +190,7 @@ __device__ __forceinline__ void tma_plain_body(const Phys& ph, const Sweep& sw, 
     for (int q = 0; q < S1; ++q) {
       if (!slot_ok<N, R, N1, S1>(q)) break;
       int l, lane;
-      slot<AX, L>(threadIdx.x + q * T, N1, l, lane);
+      slot<AX, L, T>(threadIdx.x + q * T, N1, l, lane);
 #pragma unroll
       for (int b = 0; b < N2; ++b) {
         const C x = stage[(lane + N1 * b) * L + l];
