@@ -622,8 +622,9 @@ def batched_leg():
             "criterion": "|E_k - E_{k-10}| / (10 |E_k|) < 1e-9 or 5000 steps"}
 
 
-# concurrent imaginary-time solves in the serving leg: 8 finished sooner than
-# admitting every arrival (p50 4.3 s vs 5.3 s) at ~5% less throughput
+# requests running at once in the serving leg (solves and segments, admitted in
+# arrival order): 8 kept the median near first come, first served; 4 lost
+# throughput (6.13 vs 6.49 solves/s on the 1000-request stream)
 SERVE_MAX_ACTIVE = 8
 
 

@@ -73,6 +73,7 @@ SIGNATURES = {
     "gpe_batch_bind": [_vp, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int), _vp],
     "gpe_batch_step": [_vp, ctypes.c_int, _vp],
     "gpe_batch_diagnostics": [_vp, _dp, _vp],
+    "gpe_batch_run": [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_longlong, _vp, _vp, _dp, _dp, _vp],
     "gpe_batch_set_step": [_vp, ctypes.c_int, ctypes.c_longlong],
     "gpe_batch_get_step": [_vp, ctypes.c_int, _llp],
     "gpe_batch_launch_count": [_vp, _llp],

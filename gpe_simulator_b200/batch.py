@@ -157,6 +157,23 @@ class Batch:
             self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream()))
         return out
 
+    def run(self, chunk, nchunks, tol, max_steps, live, steps, e_last):
+        """Up to ``nchunks`` chunks of ``chunk`` imaginary-time steps with the
+        convergence test on the device and one synchronisation (``gpe_batch_run``).
+        ``live`` (int32), ``steps`` (int64) and ``e_last`` (float64), one entry per
+        instance slot, are updated in place; returns the ``(count, 6)`` diagnostics
+        at each bound instance's last check (NaN for unbound slots)."""
+        n = len(self.instances)
+        assert live.dtype == np.int32 and steps.dtype == np.int64 and e_last.dtype == np.float64
+        assert live.shape == steps.shape == e_last.shape == (n,)
+        assert live.flags.c_contiguous and steps.flags.c_contiguous and e_last.flags.c_contiguous
+        out = np.full((n, 6), np.nan)
+        dp = ctypes.POINTER(ctypes.c_double)
+        _lib.check(self.lib.gpe_batch_run(
+            self._h, int(chunk), int(nchunks), float(tol), int(max_steps), live.ctypes.data, steps.ctypes.data,
+            e_last.ctypes.data_as(dp), out.ctypes.data_as(dp), _stream()))
+        return out
+
     def set_step(self, index, step):
         """Clock of real-time instance ``index``: steps taken (its next step evaluates
         the beam at ``step * dt + dt/2``)."""
@@ -172,34 +189,33 @@ class Batch:
         _lib.check(self.lib.gpe_batch_launch_count(self._h, ctypes.byref(out)))
         return out.value
 
-    def solve(self, psis, tol=1e-9, max_steps=5000, check_every=10):
-        """Run every instance to ``|dE|/E < tol`` per step or ``max_steps``.
+    def solve(self, psis, tol=1e-9, max_steps=5000, check_every=10, checks_per_call=8):
+        """Run every instance to ``|dE|/E < tol`` per step (checked every
+        ``check_every`` steps) or ``max_steps`` (a multiple of ``check_every``).
 
-        Returns ``(steps, energies)``: steps taken and final diagnostics per instance.
+        The checks run on the device (:meth:`run`), ``checks_per_call`` of them
+        per synchronisation; converged instances stop at their check and leave
+        the batch at the next rebind (when a quarter of the bound ones have
+        stopped).  Returns ``(steps, energies)``: steps taken and final
+        diagnostics per instance.
         """
+        if max_steps % check_every:
+            raise ValueError("max_steps must be a multiple of check_every")
         count = len(self.instances)
         self.bind(psis, np.ones(count, np.int32))
         steps = np.zeros(count, np.int64)
-        last = self.diagnostics()[:, 4]
-        done = np.zeros(count, bool)
+        e_last = self.diagnostics()[:, 4].copy()
+        live = np.ones(count, np.int32)
         final = np.full((count, 6), np.nan)
-        while not done.all():
-            chunk = int(min(check_every, max_steps - steps[~done].max()))
-            if chunk <= 0:
-                break
-            self.step(chunk)
-            steps[~done] += chunk
-            diag = self.diagnostics()
-            e = diag[:, 4]
-            with np.errstate(invalid="ignore", divide="ignore"):
-                rate = np.abs(e - last) / (chunk * np.abs(e))
-            newly = (~done) & ((rate < tol) | (steps >= max_steps))
-            final[newly] = diag[newly]
-            last = np.where(done, last, e)
-            if newly.any():
-                done |= newly
-                if not done.all():
-                    self.bind(self.psis, (~done).astype(np.int32))
+        bound = count
+        while live.any():
+            was = live.copy()
+            diag = self.run(check_every, checks_per_call, tol, max_steps, live, steps, e_last)
+            stopped = (was == 1) & (live == 0)
+            final[stopped] = diag[stopped]
+            if live.any() and bound - int(live.sum()) >= max(1, bound // 4):
+                self.bind(self.psis, live.copy())
+                bound = int(live.sum())
         return steps, final
 
 

@@ -941,6 +941,7 @@ __device__ __forceinline__ void fast_batch_body(const Phys* __restrict__ phs, co
     sw = sws[blockIdx.y];
   }
   __syncthreads();
+  if (batch_frozen(sw.live)) return;
   fast_body<N, AX, R, MODE>(ph, sw, op, blockIdx.x, gridDim.x);
 }
 

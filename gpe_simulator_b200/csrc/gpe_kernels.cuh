@@ -78,7 +78,18 @@ struct Sweep {
   int nbins;             // diag k-space: number of shells
   double shell_w;        // shell width
   double* hist;          // per-block shell histograms [gridDim][nbins]
+  const int* live;       // batched imaginary-time instance: 0 = frozen (converged), its
+                         // launches return at once; null: always advance
 };
+
+// A batched launch's instance is frozen: thread 0 reads the flag (written by an
+// earlier launch on the stream) into shared memory; every thread returns alike.
+__device__ __forceinline__ bool batch_frozen(const int* live) {
+  __shared__ int s_live;
+  if (threadIdx.x == 0) s_live = live ? __ldcg(live) : 1;
+  __syncthreads();
+  return s_live == 0;
+}
 
 // Values of a line program's slots (its time-dependent subexpressions, FP64,
 // evaluated on the host) at the two half-step times of one z sweep.
@@ -580,6 +591,7 @@ __global__ void __launch_bounds__(512, 1) k_sweep_batch(const Phys* __restrict__
     sw = sws[blockIdx.y];
   }
   __syncthreads();
+  if (batch_frozen(sw.live)) return;
   sweep_body<R, AX, EPT, GEN>(ph, sw);
 }
 

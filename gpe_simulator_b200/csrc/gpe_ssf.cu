@@ -395,14 +395,18 @@ __global__ void __launch_bounds__(256) k_scale(Sweep sw, long long count) {
 // batched: blockIdx.y selects the instance
 template <typename R>
 __global__ void __launch_bounds__(256) k_scale_batch(const Sweep* __restrict__ sws, long long count) {
+  if (batch_frozen(sws[blockIdx.y].live)) return;
   scale_state<R>((typename Cx<R>::T*)sws[blockIdx.y].dst, count, sws[blockIdx.y].scale);
 }
 
 // Batched finish: block b sums the partials of instance jobs[b] into out[4*index].
+// The constants give the instance's energy from its sums (as diag_scalars does).
 struct DiagJob {
   const double* pa;
   const double* pb;
   int na, nb, index;
+  int imag;                       // imaginary-time instance (takes part in convergence)
+  double ckin, dx3, inv_m, beta;
 };
 
 // Real-time batch groups: member q takes entry tick[q] of the call's time table
@@ -438,6 +442,36 @@ __global__ void k_finish_diag_batch(const DiagJob* jobs, double* out) {
   block_merge<4>(a, sh);
   if (threadIdx.x == 0)
     for (int v = 0; v < 4; ++v) out[4 * j.index + v] = a[v].value();
+}
+
+// On-device convergence of batched imaginary-time solves, after each chunk's
+// diagnostics: a live instance advances its step count by the chunk, forms its
+// energy from the finished sums exactly as the host does (same operations, no
+// contraction), and freezes when |E - E_last| / (chunk |E|) < tol (false for a
+// NaN E_last: no first-check convergence) or its steps reach max_steps.  The
+// rule of Batch.solve and of one solve at a time (checks every `chunk` steps).
+__global__ void k_batch_converge(const DiagJob* jobs, int njobs, const double* sums, int chunk, double tol,
+                                 long long max_steps, int* live, long long* steps, double* e_last) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs) return;
+  const DiagJob jb = jobs[j];
+  const int i = jb.index;
+  if (!jb.imag || !live[i]) return;
+  const double* h = sums + 4 * i;
+  const double e_kin = __dmul_rn(__dmul_rn(__dmul_rn(jb.ckin, h[3]), jb.dx3), jb.inv_m);
+  const double e_pot = __dmul_rn(h[1], jb.dx3);
+  const double e_int = __dmul_rn(__dmul_rn(__dmul_rn(0.5, jb.beta), h[2]), jb.dx3);
+  const double e = __dadd_rn(__dadd_rn(e_kin, e_pot), e_int);
+  const long long s = steps[i] + chunk;
+  const double rate = __ddiv_rn(fabs(__dsub_rn(e, e_last[i])), __dmul_rn((double)chunk, fabs(e)));
+  steps[i] = s;
+  e_last[i] = e;
+  if (rate < tol || s >= max_steps) live[i] = 0;
+}
+
+__global__ void k_fill_int(int* a, int n, int v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
 }
 
 // ---------------------------------------------------------------- image projections
@@ -1674,6 +1708,14 @@ struct gpe_batch {
   DiagJob* d_jobs = nullptr;      // finish jobs of the bound instances
   double* d_sums = nullptr;       // 4 doubles per instance
   int jobs = 0, jobs_cap = 0, sums_cap = 0;
+  // on-device convergence (gpe_batch_run): per-instance live flag (read by every
+  // batched launch of an imaginary-time instance; 1 outside gpe_batch_run), steps
+  // and last energy, with pinned staging for the caller's copies
+  int* d_live = nullptr;
+  long long* d_steps = nullptr;
+  double* d_elast = nullptr;
+  void* h_run = nullptr;
+  int live_cap = 0;
 };
 
 namespace {
@@ -1758,6 +1800,10 @@ void batch_free(gpe_batch* b) {
   if (b->h_sums) cudaFreeHost(b->h_sums);
   if (b->d_jobs) cudaFree(b->d_jobs);
   if (b->d_sums) cudaFree(b->d_sums);
+  if (b->d_live) cudaFree(b->d_live);
+  if (b->d_steps) cudaFree(b->d_steps);
+  if (b->d_elast) cudaFree(b->d_elast);
+  if (b->h_run) cudaFreeHost(b->h_run);
   for (auto* p : b->plans)
     if (p) free_plan(p);
   for (auto* p : b->parked) free_plan(p);
@@ -1915,6 +1961,7 @@ int group_upload(gpe_batch* b, gpe_batch::Group& g) {
     hph[q] = p->ph;
     for (int role = 0; role < ROLE_COUNT; ++role) {
       Sweep s = role_sweep(role, b->psis[g.members[q]], p);
+      if (g.kind == GPE_IMAGINARY && b->d_live) s.live = b->d_live + g.members[q];
       if (g.kind == GPE_REAL && role == ROLE_DZ) {
         // diagnostics at the instance's current time (the clock kernel keeps it current)
         s.t1 = s.t2 = (double)b->clock[g.members[q]] * p->dt;
@@ -1945,6 +1992,11 @@ int jobs_upload(gpe_batch* b) {
       j.pb = p->d_partial + 4 * (size_t)p->max_tiles;
       diag_tiles(p, diag_fast(p, false), j.na, j.nb);
       j.index = i;
+      j.imag = p->kind == GPE_IMAGINARY;
+      j.ckin = p->ckin;
+      j.dx3 = p->ph.dx3;
+      j.inv_m = p->ph.inv_m;
+      j.beta = p->beta;
       jobs.push_back(j);
     }
   b->jobs = (int)jobs.size();
@@ -1963,6 +2015,34 @@ int jobs_upload(gpe_batch* b) {
   }
   if (b->jobs) {
     CU(cudaMemcpyAsync(b->d_jobs, jobs.data(), sizeof(DiagJob) * b->jobs, cudaMemcpyHostToDevice, b->cap));
+    CU(cudaStreamSynchronize(b->cap));
+  }
+  return GPE_OK;
+}
+
+// Live flags (and the run state arrays) for `count` slots, every flag 1.  The
+// arrays move only here, before the groups' descriptors are rebuilt by the bind.
+int live_reset(gpe_batch* b, int count) {
+  if (count > b->live_cap) {
+    const int cap = std::max(count, 2 * b->live_cap);
+    if (b->d_live) cudaFree(b->d_live);
+    if (b->d_steps) cudaFree(b->d_steps);
+    if (b->d_elast) cudaFree(b->d_elast);
+    if (b->h_run) cudaFreeHost(b->h_run);
+    b->d_live = nullptr;
+    b->d_steps = nullptr;
+    b->d_elast = nullptr;
+    b->h_run = nullptr;
+    b->live_cap = 0;
+    CU(cudaMalloc(&b->d_live, sizeof(int) * cap));
+    CU(cudaMalloc(&b->d_steps, sizeof(long long) * cap));
+    CU(cudaMalloc(&b->d_elast, sizeof(double) * cap));
+    CU(cudaMallocHost(&b->h_run, (sizeof(int) + sizeof(long long) + sizeof(double) + 4 * sizeof(double)) * cap));
+    b->live_cap = cap;
+  }
+  if (count > 0) {
+    k_fill_int<<<(count + 255) / 256, 256, 0, b->cap>>>(b->d_live, count, 1);
+    CU(cudaGetLastError());
     CU(cudaStreamSynchronize(b->cap));
   }
   return GPE_OK;
@@ -2086,6 +2166,7 @@ int gpe_batch_bind(gpe_batch* b, void* const* psis, const int* active, void* str
       g.priority = priority;
     }
   for (int i = 0; i < count; ++i) b->psis[i] = b->plans[i] ? psis[i] : nullptr;
+  TRY(live_reset(b, count));
   for (auto& g : b->groups) {
     g.members.clear();
     for (int i : g.all)
@@ -2159,6 +2240,94 @@ int gpe_batch_diagnostics(gpe_batch* b, double* scalars, void* stream) {
   CU(cudaStreamSynchronize(st));
   for (auto& g : b->groups)
     for (int i : g.members) diag_scalars(b->plans[i], b->h_sums + 4 * i, scalars + 6 * i);
+  return GPE_OK;
+}
+
+// Chunks of imaginary-time steps with the convergence test on the device: per
+// chunk, every live bound instance takes `chunk` steps (the first without a
+// pending scale, the rest through the step graph), its lagged renormalisation,
+// the diagnostic sweeps and the finish, then k_batch_converge freezes the
+// instances that converged.  One synchronisation per call; the per-chunk work
+// is that of gpe_batch_step(chunk) + gpe_batch_diagnostics, so results are the
+// same bit for bit as a host loop over those calls that stops each instance at
+// its check.
+int gpe_batch_run(gpe_batch* b, int chunk, int nchunks, double tol, long long max_steps, int* live,
+                  long long* steps, double* e_last, double* scalars, void* stream) {
+  if (!b || !live || !steps || !e_last || !scalars) return fail(GPE_ERR_ARG, "null argument");
+  if (chunk <= 0 || nchunks <= 0 || max_steps <= 0) return fail(GPE_ERR_ARG, "chunk, nchunks and max_steps must be > 0");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = (int)b->plans.size();
+  bool any = false;
+  for (auto& g : b->groups) {
+    if (g.members.empty()) continue;
+    if (g.kind != GPE_IMAGINARY)
+      return fail(GPE_ERR_ARG, "gpe_batch_run advances imaginary-time instances only (use gpe_batch_step)");
+    if (g.uploaded != (int)g.members.size())
+      return fail(GPE_ERR_ARG, "batch membership changed without gpe_batch_bind");
+    any = true;
+  }
+  if (!any || !b->jobs) return GPE_OK;
+  if (n > b->live_cap) return fail(GPE_ERR_ARG, "batch instances added without gpe_batch_bind");
+  // the caller's state of the slots into the device arrays (through pinned staging)
+  int* h_live = (int*)b->h_run;
+  long long* h_steps = (long long*)(h_live + b->live_cap);
+  double* h_elast = (double*)(h_steps + b->live_cap);
+  double* h_sums = h_elast + b->live_cap;
+  for (int i = 0; i < n; ++i) {
+    h_live[i] = live[i] ? 1 : 0;
+    h_steps[i] = steps[i];
+    h_elast[i] = e_last[i];
+  }
+  CU(cudaMemcpyAsync(b->d_live, h_live, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(b->d_steps, h_steps, sizeof(long long) * n, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(b->d_elast, h_elast, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  if (chunk > 1 && !b->graph) {
+    CU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    const int rc = batch_step_all(b, true, b->cap);
+    cudaGraph_t gdef = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->cap, &gdef);
+    if (rc != GPE_OK) { if (gdef) cudaGraphDestroy(gdef); return rc; }
+    CU(e);
+    b->graph_def = gdef;
+    CU(cudaGraphInstantiate(&b->graph, gdef, 0));
+  }
+  for (int c = 0; c < nchunks; ++c) {
+    TRY(batch_step_all(b, false, st));
+    for (int s = 1; s < chunk; ++s) CU(cudaGraphLaunch(b->graph, st));
+    CU(cudaEventRecord(b->fork, st));
+    for (auto& g : b->groups) {
+      if (g.members.empty()) continue;
+      CU(cudaStreamWaitEvent(g.stream, b->fork, 0));
+      TRY(group_role(b, g, ROLE_SC, g.stream));
+      TRY(group_role(b, g, ROLE_DZ, g.stream));
+      TRY(group_role(b, g, ROLE_DY, g.stream));
+      TRY(group_role(b, g, ROLE_DX, g.stream));
+      CU(cudaEventRecord(g.ev, g.stream));
+      CU(cudaStreamWaitEvent(st, g.ev, 0));
+    }
+    k_finish_diag_batch<<<b->jobs, 256, 0, st>>>(b->d_jobs, b->d_sums);
+    CU(cudaGetLastError());
+    k_batch_converge<<<(b->jobs + 127) / 128, 128, 0, st>>>(b->d_jobs, b->jobs, b->d_sums, chunk, tol, max_steps,
+                                                            b->d_live, b->d_steps, b->d_elast);
+    CU(cudaGetLastError());
+    b->launches += 2;
+  }
+  CU(cudaMemcpyAsync(h_live, b->d_live, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(h_steps, b->d_steps, sizeof(long long) * n, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(h_elast, b->d_elast, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(h_sums, b->d_sums, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, st));
+  // every flag back to 1 (gpe_batch_step advances every bound instance)
+  k_fill_int<<<(n + 255) / 256, 256, 0, st>>>(b->d_live, n, 1);
+  CU(cudaGetLastError());
+  ++b->launches;
+  CU(cudaStreamSynchronize(st));
+  for (auto& g : b->groups)
+    for (int i : g.members) {
+      live[i] = h_live[i];
+      steps[i] = h_steps[i];
+      e_last[i] = h_elast[i];
+      diag_scalars(b->plans[i], h_sums + 4 * i, scalars + 6 * i);
+    }
   return GPE_OK;
 }
 

@@ -3,13 +3,17 @@
 Requests arrive over time (seeded Poisson process).  Each scheduling round the
 server
 
-1. admits every request that has arrived, while the device memory it needs fits
-   both the HBM budget and the memory the device reports free (queried every
-   round; requests wait in arrival order otherwise);
-2. advances all admitted work by one chunk: the imaginary-time solves as one
-   running :class:`Batch` (instances added on admission, removed on
-   convergence), and every real-time segment on its own CUDA stream, so the
-   segments and the batch overlap on the device;
+1. admits the requests that have arrived, in arrival order, while the device
+   memory a solve needs fits both the HBM budget and the memory the device
+   reports free (queried every round) and, with a window (``max_active``), while
+   fewer than that many requests run; a request that cannot start holds back
+   the ones behind it, except a real-time segment whose session is still busy
+   (its own earlier segments are ahead of it anyway);
+2. advances all admitted work: the imaginary-time solves as one running
+   :class:`Batch` (instances added on admission, removed on convergence) by
+   ``checks_per_round`` chunks with the convergence test on the device (one
+   synchronisation per round), and every real-time segment on its own CUDA
+   stream, so the segments and the batch overlap on the device;
 3. retires what finished (converged ground states, completed segments).
 
 Real-time requests continue a device-resident state: the server keeps one
@@ -119,7 +123,7 @@ class Server:
     real-time segments on per-session streams (see the module docstring)."""
 
     def __init__(self, sessions, dtype=torch.complex64, budget=150e9, chunk=20, max_active=None,
-                 mem_info=None, reserve=2 << 30, batch_priority=True):
+                 mem_info=None, reserve=2 << 30, batch_priority=True, ordered=True, checks_per_round=8):
         self.sessions = sessions
         self.dtype = dtype
         self.budget = budget
@@ -129,9 +133,19 @@ class Server:
         self.mem_info = mem_info or torch.cuda.mem_get_info
         self.reserve = reserve
         self.refused = 0       # admissions deferred because the device lacked free memory
-        # at most this many imaginary-time solves advance together (None: as many as
-        # the memory budget admits); fewer finish sooner, more share each launch
+        # at most this many requests run together (None: as many as the memory
+        # budget admits); fewer finish sooner, more share each launch.  ordered:
+        # the window counts imaginary-time solves and real-time segments alike and
+        # admission keeps arrival order, so that under overload the device works
+        # through the stream nearly first come, first served (a saturated device
+        # then finishes the median request no later than one request at a time
+        # would); otherwise the window counts solves only and segments start as
+        # soon as their session is free.
         self.max_active = max_active
+        self.ordered = ordered
+        # energy checks (chunks) per scheduling round, run on the device: more keep
+        # the device busy between host rounds, fewer admit arrivals sooner
+        self.checks_per_round = checks_per_round
         # the imaginary-time batch advances in short chunks with a host check after
         # each, so it runs ahead of the long real-time segments: on the device's
         # highest stream priority (the batch's own streams follow it), segments at
@@ -141,11 +155,19 @@ class Server:
 
     def run(self, requests):
         """Serve ``requests`` against the wall clock (arrival times are offsets from the
-        start); fills ``done_at`` (seconds since the start) and ``result``."""
+        start); fills ``done_at`` (seconds since the start) and ``result``.  The
+        imaginary-time requests share one tolerance and step cap (the batch's
+        device-side check takes one of each)."""
+        solves = [r for r in requests if r.kind == "imaginary"]
+        if len({(r.tol, r.max_steps) for r in solves}) > 1:
+            raise ValueError("imaginary-time requests of one run take one tol and max_steps")
+        if any(r.max_steps % self.chunk for r in solves):
+            raise ValueError("max_steps must be a multiple of the chunk")
+        tol, max_steps = (solves[0].tol, solves[0].max_steps) if solves else (0.0, 1)
         pending = sorted(requests, key=lambda r: r.arrival)
         queue = []
         imag = {}          # batch index -> [request, psi, last E, steps]
-        retired = []       # batch indices of solves finished this round
+        retired = []       # batch indices of solves finished since the last rebind
         real = {}          # session -> (request, completion event)
         used = 0.0
         batch = Batch([], self.dtype)
@@ -161,17 +183,24 @@ class Server:
             keep = []
             free = self.mem_info()[0] - self.reserve if queue else 0
             short = None   # a solve the device's free memory could not take this round
+            held = False   # ordered admission: an earlier request could not start
             for r in queue:
+                if held:
+                    keep.append(r)
+                    continue
+                running = len(imag) + len(real) if self.ordered else len(imag)
+                full = self.max_active is not None and running >= self.max_active
                 if r.kind == "imaginary":
                     need = state_bytes(r.inst.n, self.dtype)
-                    full = self.max_active is not None and len(imag) >= self.max_active
                     if used + need > self.budget or full:
                         keep.append(r)
+                        held = self.ordered
                         continue
                     if need > free:
                         self.refused += 1
                         short = short or (r, need)
                         keep.append(r)
+                        held = self.ordered
                         continue
                     free -= need
                     with torch.cuda.stream(self.batch_stream):
@@ -182,8 +211,9 @@ class Server:
                     changed = True
                 else:
                     sess = self.sessions[r.session]
-                    if sess.busy:
+                    if sess.busy or (self.ordered and full):
                         keep.append(r)
+                        held = self.ordered and not sess.busy
                         continue
                     sess.busy = True
                     st = self.streams[r.session]
@@ -202,33 +232,8 @@ class Server:
             if imag:
                 with torch.cuda.stream(self.batch_stream):
                     if changed:
-                        psis = [None] * len(batch.instances)
-                        act = np.zeros(len(batch.instances), np.int32)
-                        for idx, rec in imag.items():
-                            psis[idx] = rec[1]
-                            act[idx] = 1
-                        batch.bind(psis, act)
-                    batch.step(self.chunk)
-                    diag = batch.diagnostics()      # synchronises the batch stream only
-                now = clock()
-                for idx in list(imag):
-                    rec = imag[idx]
-                    r = rec[0]
-                    rec[3] += self.chunk
-                    e = diag[idx, 4]
-                    conv = abs(e - rec[2]) / (self.chunk * abs(e)) < r.tol     # NaN on the first check
-                    rec[2] = e
-                    if conv or rec[3] >= r.max_steps:
-                        r.done_at, r.taken = now, rec[3]
-                        r.result = dict(N=diag[idx, 0], E=e, mu=diag[idx, 5], psi=rec[1])
-                        used -= state_bytes(r.inst.n, self.dtype)
-                        del imag[idx]
-                        retired.append(idx)
-                if retired:
-                    # one rebind for every retirement of the round (the batch's device
-                    # tables are rebuilt once); the retired instances, no longer bound,
-                    # then leave the batch without another rebuild
-                    with torch.cuda.stream(self.batch_stream):
+                        # one rebind for the admissions and every retirement since the
+                        # last one (retired solves stayed bound, frozen, in between)
                         psis = [None] * len(batch.instances)
                         act = np.zeros(len(batch.instances), np.int32)
                         for idx, rec in imag.items():
@@ -236,8 +241,30 @@ class Server:
                             act[idx] = 1
                         batch.bind(psis, act)
                         for idx in retired:
-                            batch.remove(idx)
-                    retired.clear()
+                            batch.remove(idx)      # unbound now: leaves without a rebuild
+                        retired.clear()
+                    slots = len(batch.instances)
+                    live = np.zeros(slots, np.int32)
+                    steps = np.zeros(slots, np.int64)
+                    e_last = np.full(slots, np.nan)
+                    for idx, rec in imag.items():
+                        live[idx], steps[idx], e_last[idx] = 1, rec[3], rec[2]
+                    # checks on the device (first check of a solve: E_last NaN, no
+                    # convergence); synchronises the batch stream only
+                    diag = batch.run(self.chunk, self.checks_per_round, tol, max_steps, live, steps, e_last)
+                now = clock()
+                for idx in list(imag):
+                    rec = imag[idx]
+                    r = rec[0]
+                    rec[2], rec[3] = float(e_last[idx]), int(steps[idx])
+                    if not live[idx]:
+                        r.done_at, r.taken = now, rec[3]
+                        r.result = dict(N=diag[idx, 0], E=diag[idx, 4], mu=diag[idx, 5], psi=rec[1])
+                        used -= state_bytes(r.inst.n, self.dtype)
+                        del imag[idx]
+                        retired.append(idx)
+                # retired solves stay bound but frozen (their launches return at once)
+                # until the next admission rebinds the batch
             elif real or queue:
                 time.sleep(2e-4)
             elif pending:

@@ -219,7 +219,19 @@ int  gpe_status(gpe_plan* plan, int* flags, void* stream);
  *   gpe_batch_set_step / gpe_batch_get_step: a real-time instance's clock (steps
  *     taken; its next step evaluates the beam at t_mid = step * dt + dt/2).
  *   gpe_batch_diagnostics: scalars[6*i .. 6*i+5] = {N, E_kin, E_pot, E_int, E, mu}
- *     of every bound instance i (synchronises); real-time instances at their clock's t. */
+ *     of every bound instance i (synchronises); real-time instances at their clock's t.
+ *   gpe_batch_run: up to nchunks chunks of `chunk` imaginary-time steps with the
+ *     convergence test on the device, one synchronisation per call (the loop of
+ *     gpe/launch.py:8-13 over standard_imaginary_step with an energy check every
+ *     `chunk` steps, for many solves at once).  Per slot i, in and out: live[i]
+ *     (nonzero: still advancing), steps[i] (steps taken), e_last[i] (energy at the
+ *     previous check; NaN: the first check cannot converge).  After each chunk a
+ *     live instance adds `chunk` to steps[i], takes its energy E and stops advancing
+ *     when |E - e_last[i]| / (chunk |E|) < tol or steps[i] >= max_steps; e_last[i]
+ *     becomes E.  scalars as gpe_batch_diagnostics, at each instance's last check.
+ *     Every bound instance must be imaginary-time; frozen instances stay bound
+ *     (their launches return at once) until the caller rebinds without them.
+ *     Results equal gpe_batch_step(chunk) + gpe_batch_diagnostics per check. */
 typedef struct gpe_batch gpe_batch;
 int  gpe_batch_create(const gpe_desc* descs, int count, gpe_batch** batch);
 int  gpe_batch_destroy(gpe_batch* batch);
@@ -228,6 +240,8 @@ int  gpe_batch_remove(gpe_batch* batch, int index);
 int  gpe_batch_bind(gpe_batch* batch, void* const* psis, const int* active, void* stream);
 int  gpe_batch_step(gpe_batch* batch, int nsteps, void* stream);
 int  gpe_batch_diagnostics(gpe_batch* batch, double* scalars, void* stream);
+int  gpe_batch_run(gpe_batch* batch, int chunk, int nchunks, double tol, long long max_steps, int* live,
+                   long long* steps, double* e_last, double* scalars, void* stream);
 int  gpe_batch_set_step(gpe_batch* batch, int index, long long step);
 int  gpe_batch_get_step(const gpe_batch* batch, int index, long long* step);
 int  gpe_batch_launch_count(const gpe_batch* batch, long long* count);

@@ -81,6 +81,96 @@ def test_solve_converges_and_retires(cuda):
     np.testing.assert_allclose(final[:, 0], 1.0, atol=1e-5)
 
 
+def _host_checked_solve(b, states, tol, max_steps, chunk):
+    """The convergence loop on the host: step(chunk) + diagnostics per check,
+    converged instances unbound at once (the rule gpe_batch_run applies on the device)."""
+    count = len(states)
+    b.bind(states, np.ones(count, np.int32))
+    steps = np.zeros(count, np.int64)
+    last = b.diagnostics()[:, 4]
+    done = np.zeros(count, bool)
+    final = np.full((count, 6), np.nan)
+    while not done.all():
+        b.step(chunk)
+        steps[~done] += chunk
+        diag = b.diagnostics()
+        e = diag[:, 4]
+        with np.errstate(invalid="ignore", divide="ignore"):
+            rate = np.abs(e - last) / (chunk * np.abs(e))
+        newly = (~done) & ((rate < tol) | (steps >= max_steps))
+        final[newly] = diag[newly]
+        last = np.where(done, last, e)
+        done |= newly
+        if newly.any() and not done.all():
+            b.bind(states, (~done).astype(np.int32))
+    return steps, final
+
+
+@pytest.mark.parametrize("checks_per_call", [1, 3, 8])
+def test_device_convergence_equals_host_checks_bitwise(cuda, checks_per_call):
+    """Batch.solve with the energy checks on the device (gpe_batch_run, several
+    checks per synchronisation, converged instances frozen in place) stops every
+    instance at the same step, with the same state and diagnostics bit for bit,
+    as the host loop of step + diagnostics that unbinds each at its check."""
+    from gpe_simulator_b200.batch import Batch, initial_states
+    insts = small_batch()
+    states = initial_states(insts, torch.complex64)
+    # tolerance from a probe run: the median of the instances' rates at the last
+    # check, so that some converge before the cap and some run to it
+    probe = Batch(insts, torch.complex64)
+    c = [s.clone() for s in states]
+    probe.bind(c)
+    last = probe.diagnostics()[:, 4]
+    for _ in range(20):
+        probe.step(20)
+        e = probe.diagnostics()[:, 4]
+        rate, last = np.abs(e - last) / (20 * np.abs(e)), e
+    probe.close()
+    tol = float(np.median(rate))
+    a = [s.clone() for s in states]
+    b = [s.clone() for s in states]
+    ba = Batch(insts, torch.complex64)
+    steps_a, final_a = ba.solve(a, tol=tol, max_steps=400, check_every=20, checks_per_call=checks_per_call)
+    bb = Batch(insts, torch.complex64)
+    steps_b, final_b = _host_checked_solve(bb, b, tol=tol, max_steps=400, chunk=20)
+    torch.cuda.synchronize()
+    assert np.array_equal(steps_a, steps_b)
+    assert (steps_a < 400).any() and (steps_a == 400).any()    # some stop early, some at the cap
+    assert np.array_equal(final_a, final_b)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    ba.close()
+    bb.close()
+
+
+def test_batch_run_state_in_and_out(cuda):
+    """gpe_batch_run's per-slot state: a frozen slot stays as it is, a live one
+    advances by chunk per check, a NaN last energy blocks the first check, and the
+    step cap freezes; gpe_batch_step afterwards still advances every bound instance."""
+    from gpe_simulator_b200.batch import Batch, initial_states
+    insts = small_batch()[:3]
+    states = initial_states(insts, torch.complex64)
+    b = Batch(insts, torch.complex64)
+    b.bind(states)
+    frozen = states[1].clone()
+    live = np.array([1, 0, 1], np.int32)
+    steps = np.array([0, 7, 40], np.int64)
+    e_last = np.array([np.nan, 1.0, np.nan])
+    diag = b.run(20, 3, 1e-30, 80, live, steps, e_last)
+    torch.cuda.synchronize()
+    assert steps.tolist() == [60, 7, 80] and live.tolist() == [1, 0, 0]
+    assert e_last[1] == 1.0 and np.isfinite(e_last[[0, 2]]).all()
+    assert torch.equal(states[1], frozen)
+    assert np.isfinite(diag[[0, 2]]).all()
+    before = states[1].clone()
+    b.step(2)
+    torch.cuda.synchronize()
+    assert not torch.equal(states[1], before)
+    with pytest.raises(ValueError, match="chunk"):
+        b.run(0, 1, 1e-9, 20, live, steps, e_last)
+    b.close()
+
+
 def test_add_remove_keeps_results_identical(cuda):
     """Continuous batching: instances join and leave a running batch; every
     instance still matches its solo run bit for bit."""

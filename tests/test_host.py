@@ -270,21 +270,6 @@ def test_ctypes_signatures_match_the_header_prototypes():
                 assert t is scalar[base], (name, p, t)
 
 
-def test_integration_guide_descriptor_matches_the_library():
-    """The ctypes ``Desc`` shown in INTEGRATION.md (the stub a reference
-    maintainer would copy) has the library's field names, types and offsets."""
-    from gpe_simulator_b200 import _lib
-    doc = (Path(__file__).resolve().parents[1] / "INTEGRATION.md").read_text()
-    block = re.search(r"^class Desc\(ctypes\.Structure\):.*?\]\n", doc, re.S | re.M).group(0)
-    scope = {"ctypes": ctypes}
-    exec(block, scope)
-    Doc = scope["Desc"]
-    assert [f for f, _ in Doc._fields_] == [f for f, _ in _lib.Desc._fields_]
-    assert ctypes.sizeof(Doc) == ctypes.sizeof(_lib.Desc)
-    for (f, _), (g, _) in zip(Doc._fields_, _lib.Desc._fields_):
-        assert getattr(Doc, f).offset == getattr(_lib.Desc, g).offset, f
-
-
 def test_python_constants_match_the_header():
     """Status codes, dtype/kind/potential kinds, bytecode opcodes and projection
     bits as the Python layer spells them equal the header's #defines."""
