@@ -123,7 +123,7 @@ class Server:
     real-time segments on per-session streams (see the module docstring)."""
 
     def __init__(self, sessions, dtype=torch.complex64, budget=150e9, chunk=20, max_active=None,
-                 mem_info=None, reserve=2 << 30, batch_priority=True, ordered=True, checks_per_round=8):
+                 mem_info=None, reserve=2 << 30, batch_priority=True, ordered=True, checks_per_round=16):
         self.sessions = sessions
         self.dtype = dtype
         self.budget = budget
