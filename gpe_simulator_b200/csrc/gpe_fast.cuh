@@ -239,8 +239,10 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
 //   phase 2 (role p1 + 8 k3): DFT8 over p2 -> k1, times W_64^(p1 k1)    (twb[k1*8 + p1])
 //   phase 3 (role k3 + 8 k1): DFT8 over p1 -> k2; lane k3 + 8 k1 holds X[lane + 64 k2]
 // Exchange layouts: Z tiles (a warp per line) rows of 72 elements per (line, k),
-// the second exchange with a pitch of 9 per p1, so that 8-byte accesses of a
-// half warp avoid bank conflicts; P tiles line-fastest, [k][role][l].
+// the second exchange at 8 p1 + (k3 ^ p1) within its row, so that the 8-byte
+// accesses of a half warp avoid bank conflicts in both directions; P tiles
+// line-fastest, [k][role][l].  A thread's two slots are 32 lanes apart, so its
+// p1 is the same in both: each W_64 twiddle is loaded once for the two.
 template <int N, int AX, typename R, int Q, int V>
 __device__ __forceinline__ void fft_3phase(typename Cx<R>::T (&v)[V], typename Cx<R>::T* ex,
                                            const typename TwE<R>::T* twa, const typename TwE<R>::T* twb) {
@@ -252,7 +254,7 @@ __device__ __forceinline__ void fft_3phase(typename Cx<R>::T (&v)[V], typename C
   constexpr bool WARP_LOCAL = AX == FZ && T == 32 * L;
   auto e1 = [](int l, int k3, int p) { return AX == FZ ? (l * RD + k3) * 72 + p : (k3 * A + p) * L + l; };
   auto e2 = [](int l, int k3, int k1, int p1) {
-    return AX == FZ ? (l * RD + k1) * 72 + 9 * p1 + k3 : ((k1 * RD + k3) * RD + p1) * L + l;
+    return AX == FZ ? (l * RD + k1) * 72 + 8 * p1 + (k3 ^ p1) : ((k1 * RD + k3) * RD + p1) * L + l;
   };
   auto sync = [] { if (WARP_LOCAL) __syncwarp(); else __syncthreads(); };
 #pragma unroll
@@ -277,17 +279,27 @@ __device__ __forceinline__ void fft_3phase(typename Cx<R>::T (&v)[V], typename C
     for (int p2 = 0; p2 < RD; ++p2) x[p2] = ex[e1(l, k3, p1 + RD * p2)];
   }
   sync();
+  static_assert(T % (8 * L) == 0 || AX == FZ, "slots 32 lanes apart");
+#pragma unroll
+  for (int s = 0; s < Q; ++s) Dft<RD>::run(v + s * RD, (const C*)nullptr, (const C*)nullptr, N / RD);
+  {
+    int l0, q0;
+    slot<AX, L, T>(threadIdx.x, A, l0, q0);
+    const int p1 = q0 & 7;
+#pragma unroll
+    for (int k1 = 1; k1 < RD; ++k1) {
+      const typename TwE<R>::T w = twb[k1 * RD + p1];
+#pragma unroll
+      for (int s = 0; s < Q; ++s) v[s * RD + k1] = tw_apply(v[s * RD + k1], w);
+    }
+  }
 #pragma unroll
   for (int s = 0; s < Q; ++s) {
     int l, q;
     slot<AX, L, T>(threadIdx.x + s * T, A, l, q);
     const int p1 = q & 7, k3 = q >> 3;
-    C* x = v + s * RD;
-    Dft<RD>::run(x, (const C*)nullptr, (const C*)nullptr, N / RD);
 #pragma unroll
-    for (int k1 = 1; k1 < RD; ++k1) x[k1] = tw_apply(x[k1], twb[k1 * RD + p1]);
-#pragma unroll
-    for (int k1 = 0; k1 < RD; ++k1) ex[e2(l, k3, k1, p1)] = x[k1];
+    for (int k1 = 0; k1 < RD; ++k1) ex[e2(l, k3, k1, p1)] = v[s * RD + k1];
   }
   sync();
 #pragma unroll
