@@ -175,7 +175,7 @@ __device__ __forceinline__ void slot(int gs, int per, int& l, int& lane) {
 // One forward FFT of every line of the tile, A = lanes in phase 1 (values A-strided),
 // B = values per lane in phase 1.  In: v[s][b] = x[lane_s + A*b] of line l_s (phase-1
 // slots).  Out: v[s][a] = X[lane_s + B*a] (phase-2 slots with B lanes per line).
-template <int N, int A, int B, int AX, typename R, int QA, int QB, int V, bool ASYNC_NEXT = false>
+template <int N, int A, int B, int AX, typename R, int QA, int QB, int V, bool ASYNC_NEXT = false, bool TAIL = true>
 __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename Cx<R>::T* ex,
                                            const typename TwE<R>::T* tw) {
   // In: QA slots of (A lanes, B values), slot s holding x[lane + A*b] in v[s*B + b].
@@ -184,6 +184,8 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
   // for complex64): consecutive lanes read consecutive entries.
   // ASYNC_NEXT: the exchange buffer is overwritten by a TMA copy after the final
   // barrier, so each thread fences its exchange accesses against the async proxy.
+  // TAIL: end with a barrier that frees the exchange buffer for a next transform;
+  // the last transform of a sweep leaves it out (nothing reuses the buffer).
   using C = typename Cx<R>::T;
   constexpr int L = FastCfg<N, R>::L;
   constexpr int T = FastCfg<N, R>::T;
@@ -226,7 +228,9 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
     Dft<A>::run(x, (const C*)nullptr, (const C*)nullptr, N / A);
   }
   if (ASYNC_NEXT) fence_proxy_async_smem();
-  if (WARP_LOCAL) __syncwarp(); else __syncthreads();
+  if (TAIL) {
+    if (WARP_LOCAL) __syncwarp(); else __syncthreads();
+  }
 }
 
 // One forward FFT of every line of the tile for N = 8^3 (n = 512), in three
@@ -243,7 +247,7 @@ __device__ __forceinline__ void fft_2phase(typename Cx<R>::T (&v)[V], typename C
 // accesses of a half warp avoid bank conflicts in both directions; P tiles
 // line-fastest, [k][role][l].  A thread's two slots are 32 lanes apart, so its
 // p1 is the same in both: each W_64 twiddle is loaded once for the two.
-template <int N, int AX, typename R, int Q, int V>
+template <int N, int AX, typename R, int Q, int V, bool TAIL = true>
 __device__ __forceinline__ void fft_3phase(typename Cx<R>::T (&v)[V], typename Cx<R>::T* ex,
                                            const typename TwE<R>::T* twa, const typename TwE<R>::T* twb) {
   using C = typename Cx<R>::T;
@@ -312,7 +316,7 @@ __device__ __forceinline__ void fft_3phase(typename Cx<R>::T (&v)[V], typename C
     for (int p1 = 0; p1 < RD; ++p1) x[p1] = ex[e2(l, k3, k1, p1)];
     Dft<RD>::run(x, (const C*)nullptr, (const C*)nullptr, N / RD);
   }
-  sync();
+  if (TAIL) sync();   // frees the exchange buffer for a next transform
 }
 
 template <typename R>
@@ -876,14 +880,16 @@ __device__ __forceinline__ void fast_body(const Phys& ph, const Sweep& sw, const
   __syncthreads();  // twiddles and tables visible
   if (MODE == FM_Z1) fast_pointwise<N, AX, R, MODE, 0, N1, N2, S1>(v, tl, ph, tb, op, cx);
   if (MODE == FM_DIAGR) diag_real_all<N, AX, R, N1, N2, S1>(v, tl, ph, tb, cx);
-  if constexpr (THREE) fft_3phase<N, AX, R, S1, EPT>(v, ex, t1, t2);
-  else fft_2phase<N, N1, N2, AX, R, S1, S2, EPT>(v, ex, t1);
+  // the first transform frees the exchange buffer only when a second one follows
+  constexpr bool TWO_FFT = MODE == FM_Z21 || MODE == FM_XKIN;
+  if constexpr (THREE) fft_3phase<N, AX, R, S1, EPT, TWO_FFT>(v, ex, t1, t2);
+  else fft_2phase<N, N1, N2, AX, R, S1, S2, EPT, false, TWO_FFT>(v, ex, t1);
   if (MODE == FM_Z21 || MODE == FM_XKIN) {
     if (MODE == FM_Z21) conj_all(v);  // finish the inverse before the physics
     fast_pointwise<N, AX, R, MODE, 1, LM, VM, SM>(v, tl, ph, tb, op, cx);
     if (MODE == FM_XKIN) conj_all(v);  // start the inverse
-    if constexpr (THREE) fft_3phase<N, AX, R, S1, EPT>(v, ex, t1, t2);
-    else fft_2phase<N, N2, N1, AX, R, S2, S1, EPT>(v, ex, t2);
+    if constexpr (THREE) fft_3phase<N, AX, R, S1, EPT, false>(v, ex, t1, t2);
+    else fft_2phase<N, N2, N1, AX, R, S2, S1, EPT, false, false>(v, ex, t2);
     if (MODE == FM_XKIN) conj_all(v);
     fast_store<N, AX, R, N1, N2, S1>(v, tl, (C*)sw.dst);
   } else {
